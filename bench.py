@@ -1,0 +1,450 @@
+#!/usr/bin/env python
+"""Benchmark of the exact big-integer matrix product on B200.
+
+One step = one pass of the whole pipeline (split + forward NTT, contraction,
+inverse NTT, CRT + recompose) over one batch of the workload.  Default
+workload: 4096 independent products, m,k,n uniform in {2..16}, signed entries
+with bit lengths log-uniform in [2^10, 2^18] (seeded synthetic inputs).
+
+  value      products/s with inputs resident in HBM (device-timed, CUDA events)
+  e2e        products/s through the public C ABI (mpzmm_matmul_batch) with
+             host buffers: host->device copy of the inputs and device->host
+             copy of the results inside the timed region
+  roofline   the dominant stage: algorithmic bytes / its event-timed duration
+  cpu_baseline  the reference's own CPU mpz_rmatrix_mult_fft (oracle/_ref) on
+             a bounded sample of the same workload, on this host's cores
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "bit-exact mpz matmuls/s (4096-product batch, m,k,n in 2..16, 2^10..2^18-bit signed)"
+UNIT = "products/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["config3", "config2", "config4", "config1"],
+                    default="config3")
+    ap.add_argument("--count", type=int, default=4096, help="products per batch (config3)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", type=int, default=256,
+                    help="products in the CPU-baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-verify", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_workload(name, replicate, count):
+    from rforest_b200 import workloads as W
+    if name == "config3":
+        return W.config3(replicate, count=count)
+    if name == "config2":
+        return [W.config2(replicate)]
+    if name == "config4":
+        return [W.config4(replicate)]
+    return [W.config1(replicate)]
+
+
+def workload_config(name, count):
+    if name == "config3":
+        return {"workload": "batched exact matmul", "products_per_step": count,
+                "dims": "m,k,n uniform in {2..16}", "bits": "log-uniform [2^10, 2^18], signed",
+                "seed": "3000 + replicate"}
+    if name == "config2":
+        return {"workload": "single 8x8x8 exact matmul", "products_per_step": 1,
+                "bits": "65536, signed", "seed": 2001}
+    if name == "config4":
+        return {"workload": "single 64x64x64 exact matmul", "products_per_step": 1,
+                "bits": "2^20, unsigned", "seed": 4001}
+    return {"workload": "single 4x4x4 exact matmul", "products_per_step": 1,
+            "bits": "4096, signed", "seed": 1001}
+
+
+# Algorithmic bytes of the 3-pass model at the reference's own parameters
+# (4 primes, 64-bit residues, N = 2^lgN from its GPU parameter choice,
+# src/lib/mpnfft.c:664-708):  R = 8 * 4 * N bytes per polynomial.
+_REF_PRIMES = [0x3fffc00000000001, 0x3ffdf00000000001, 0x3ffd900000000001,
+               0x3ffd500000000001]
+
+
+def reference_lgN(maxlimbs: int, terms: int) -> int:
+    bits = 64 * (2 * maxlimbs + 1)
+    bound = 0.4999
+    for p in _REF_PRIMES:
+        bound *= float(p)
+    bound2 = bound / terms
+    r = 62 * 4 // 2
+    while True:
+        points = (bits - 1) // r + 2
+        thing = bound2 / ((points + 1) // 2)
+        _, e = math.frexp(thing)
+        rr = (e - 1) // 2
+        if rr == r:
+            return max(0, (points - 1).bit_length())
+        r = rr
+
+
+def pass_bytes(prods, out_limbs_per_product):
+    """(pass1, pass2, pass3) algorithmic bytes summed over the batch."""
+    b1 = b2 = b3 = 0
+    for p, lc in zip(prods, out_limbs_per_product):
+        la = int(p.A.nlimbs.sum())
+        lb = int(p.B.nlimbs.sum())
+        maxl = max(p.A.max_limbs(), p.B.max_limbs())
+        N = 1 << reference_lgN(maxl, p.k)
+        R = 8 * 4 * N
+        nin = p.m * p.k + p.k * p.n
+        nout = p.m * p.n
+        b1 += 8 * (la + lb) + R * nin
+        b2 += R * nin + R * nout
+        b3 += R * nout + 8 * lc
+    return b1, b2, b3
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.path = os.path.join(ROOT, "_work", f".clocks_{os.getpid()}.csv")
+        self.dev = device_index
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append(parts)
+                except ValueError:
+                    pass
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU path on this host's cores
+# ---------------------------------------------------------------------------
+def _cpu_worker(args):
+    name, replicate, indices = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from rforest_b200 import workloads as W
+    if name == "config3":
+        prods = [W.random_product(3000 + replicate, t, 2, 16, 10, 18) for t in indices]
+    else:
+        prods = make_workload(name, replicate, 1)
+    t0 = time.perf_counter()
+    for p in prods:
+        O.matmul_reference(p.m, p.k, p.n, p.A, p.B)
+    return time.perf_counter() - t0, len(prods)
+
+
+def cpu_reference_rate(name, replicate, sample, workers, pool=None):
+    """Products/s of the reference CPU path on `sample` products, `workers`
+    processes (the reference is single-threaded)."""
+    from oracle import oracle as O
+    kind = "reference" if O.reference_available() else None
+    if kind is None:
+        raise RuntimeError("oracle/_ref is not built")
+    n = sample if name == "config3" else 1
+    chunks = [list(range(i, n, workers)) for i in range(min(workers, n))]
+    t0 = time.perf_counter()
+    if pool is None or len(chunks) == 1:
+        res = [_cpu_worker((name, replicate, c)) for c in chunks]
+    else:
+        res = pool.map(_cpu_worker, [(name, replicate, c) for c in chunks])
+    wall = time.perf_counter() - t0
+    done = sum(r[1] for r in res)
+    return done / wall, len(chunks), done
+
+
+def cpu_workers():
+    n = os.cpu_count() or 1
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return max(1, min(n, 64))
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    workers = cpu_workers()
+    ctx = mp.get_context("spawn")
+    sample = args.cpu_sample
+    with ctx.Pool(workers) as pool:
+        for _ in range(args.warmup):
+            cpu_reference_rate(args.workload, 1, min(sample, workers), workers, pool)
+        rates = []
+        t0 = time.perf_counter()
+        done_total = 0
+        for _ in range(args.steps):
+            rate, used, done = cpu_reference_rate(args.workload, 1, sample, workers, pool)
+            rates.append(rate)
+            done_total += done
+        wall = time.perf_counter() - t0
+    value = done_total / wall
+    cfg = workload_config(args.workload, args.count)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": dict(cfg, sample_products_per_step=sample if args.workload == "config3" else 1,
+                       cpu_note="reference API is r x d by d x d: shapes zero-padded to "
+                                "d = max(k, n)"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference",
+                         "sample": f"first {sample} products of the batch per step, "
+                                   f"{used} worker processes"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import multiprocessing as mp
+    cpu_pool = None
+    workers = cpu_workers()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # spawn the CPU pool before the first GPU call
+        cpu_pool = mp.get_context("spawn").Pool(workers)
+
+    import torch
+    import torch.distributed as dist
+    from rforest_b200 import api, packed as PK
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    api.setup(local_rank)
+    stream = torch.cuda.Stream()
+
+    replicate = 1 + rank
+    prods = make_workload(args.workload, replicate, args.count)
+    units_per_rank = len(prods)
+    triples = [(p.m, p.k, p.n, p.A, p.B) for p in prods]
+
+    # ---- device-resident throughput ----
+    plan = api.Plan(triples, stream=stream)
+    info = plan.info(0)
+    for _ in range(args.warmup):
+        plan.execute(stream)
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    plan.set_timing(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    plan.set_timing(False)
+    ms = ev0.elapsed_time(ev1)
+    stage_ms, stage_launches, timed = plan.stage_times()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = units_per_rank * world * args.steps / (ms / 1000.0)
+
+    outs = plan.download(stream)
+    out_limbs = [int(np.abs(c.sizes.astype(np.int64)).sum()) for c in outs]
+    verified = None
+    if not args.no_verify:
+        verified = verify(args.workload, replicate, outs)
+    plan.close()
+    del plan
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e_steps = max(1, args.e2e_steps)
+    batch = api.Batch(triples)
+    batch.run(stream=stream)  # warm the library's workspace and the output pages
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        batch.run(stream=stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = units_per_rank * world * e2e_steps / (e2e_ms / 1000.0)
+    h2d = sum(int(p.A.nlimbs.sum() + p.B.nlimbs.sum()) * 8 for p in prods)
+    d2h_words = 0
+    for p in prods:
+        cap = api.output_limbs(p.k, 64 * p.A.max_limbs(), 64 * p.B.max_limbs())
+        d2h_words += p.m * p.n * cap
+    d2h = d2h_words * 8
+
+    if rank == 0:
+        # roofline of the dominant stage (3-pass model, reference parameters)
+        b1, b2, b3 = pass_bytes(prods, out_limbs)
+        names = ["split_fwd_ntt", "contract", "inv_ntt", "crt_recompose"]
+        dom = int(np.argmax(stage_ms))
+        if dom == 0:
+            alg, t_ms, kern = b1, stage_ms[0], "k_split_fwd"
+        elif dom == 1:
+            alg, t_ms, kern = b2, stage_ms[1], "k_contract"
+        else:
+            alg, t_ms, kern = b3, stage_ms[2] + stage_ms[3], "k_inv_ntt+k_crt_recompose"
+        peaks = load_peaks()
+        per_launch_s = (t_ms / 1000.0) / max(1, timed)
+        achieved = alg / per_launch_s / 1e9
+        cpu = None
+        if cpu_pool is not None:
+            rate, used, done = cpu_reference_rate(args.workload, 1, args.cpu_sample, workers,
+                                                  cpu_pool)
+            cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "reference",
+                   "sample": f"first {done} products of the batch, reference CPU "
+                             f"mpz_rmatrix_mult_fft, {used} worker processes"}
+            cpu_pool.close()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": dict(workload_config(args.workload, args.count),
+                           l2="inputs larger than L2 (residues of the batch >> 126 MB)",
+                           params_product0=info, device_bytes=info["device_bytes"],
+                           e2e_steps=e2e_steps, parallelism=f"replicas x{world}"),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(sum(stage_launches) * args.steps),
+            "stages_ms_per_step": {n: round(t / max(1, timed), 4)
+                                   for n, t in zip(names, stage_ms)},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved,
+                         "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+                         "peak_source": peaks[1], "traffic": None,
+                         "alg_bytes_per_step": alg},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "verified": verified,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (of fallback)"
+
+
+def verify(name, replicate, outs):
+    """Digest check against the reference's golden outputs where they exist."""
+    from rforest_b200 import packed as PK
+    path = os.path.join(ROOT, "tests", "golden", "digests.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+    except OSError:
+        return None
+    if replicate != 1:
+        return None
+    if name == "config3" and "config3" in d:
+        want = d["config3"]["C"]
+        n = min(len(want), len(outs))
+        return all(PK.digest(outs[t]) == want[t] for t in range(n))
+    key = {"config1": "config1", "config2": "config2", "config4": "config4"}.get(name)
+    if key and key in d:
+        return PK.digest(outs[0]) == d[key]["C"]
+    return None
+
+
+if __name__ == "__main__":
+    main()

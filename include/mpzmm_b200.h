@@ -1,0 +1,182 @@
+/*
+ * mpzmm_b200 -- exact big-integer matrix product on one B200 (sm_100a).
+ *
+ * C ABI of libmpzmm_b200.so.  Two layers:
+ *
+ *  1. Drop-in replacements for the reference's public matmul API
+ *     (alexp616/rforest src/include/hwmpz.h), same names and signatures, so
+ *     rforest links this library in place of src/lib/hwmpz.c.
+ *  2. Status-returning entry points over plain arrays ("packed vectors",
+ *     below) for general m x k by k x n shapes, batches of independent
+ *     products, device-resident plans, and a serving queue.  They have no
+ *     counterpart in the reference, which reports no errors
+ *     (src/lib/hwmpz.c:69,146 use assert / exit).
+ *
+ * Packed vector: entry e has |sizes[e]| 64-bit limbs, least significant
+ * first, at limbs[offs[e]], and the sign of sizes[e] -- GMP's own
+ * (_mp_size, _mp_d) convention.  Matrices are row-major.
+ *
+ * All arithmetic is exact integer arithmetic on the GPU; there is no CPU
+ * fallback.  Without a usable CUDA device every compute entry point returns
+ * MPZMM_ERR_CUDA (the void reference-compatible ones call the fatal hook).
+ */
+#ifndef MPZMM_B200_H
+#define MPZMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "mpzmm_gmp_abi.h"
+
+#if defined(__GNUC__)
+#define MPZMM_API __attribute__((visibility("default")))
+#else
+#define MPZMM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define MPZMM_OK 0
+#define MPZMM_ERR_ARG 1        /* malformed dimensions or pointers        */
+#define MPZMM_ERR_TOO_LARGE 2  /* product exceeds the supported size      */
+#define MPZMM_ERR_CAPACITY 3   /* an output capacity is too small         */
+#define MPZMM_ERR_CUDA 4       /* CUDA runtime failure / no device        */
+#define MPZMM_ERR_NOMEM 5      /* host or device allocation failed        */
+#define MPZMM_ERR_STATE 6      /* not set up, or object in the wrong state */
+#define MPZMM_ERR_TIMEOUT 7    /* a bounded wait gave up                  */
+#define MPZMM_ERR_BUSY 8       /* admission refused (queue/memory full)   */
+
+/* ======================================================================
+ * 1. Reference-compatible API (src/include/hwmpz.h)
+ * ====================================================================== */
+
+/* Replaces hw_mpz_setup (src/include/hwmpz.h:74, src/lib/hwmpz.c:51):
+   selects the CUDA device (MPZMM_DEVICE env, default 0), builds prime and
+   twiddle tables on it.  Idempotent. */
+MPZMM_API void hw_mpz_setup(void);
+/* Replaces hw_mpz_clear (src/include/hwmpz.h:75, src/lib/hwmpz.c:52). */
+MPZMM_API void hw_mpz_clear(void);
+
+/* Replaces mpz_rmatrix_mult_fft (src/include/hwmpz.h:127-129,
+   src/lib/hwmpz.c:65-130): C = A * B exactly, A r x d, B d x d, C r x d,
+   row-major mpz_t arrays.  C entries must be initialised; they are grown with
+   GMP's mpz_realloc (so a caller-installed GMP allocator is honoured).
+   w is unused, as in the reference.  No aliasing of C with A or B.
+   Errors call mpzmm_fatal (see mpzmm_set_fatal_hook). */
+MPZMM_API void mpz_rmatrix_mult_fft(mpz_t *C, mpz_t *A, int r, mpz_t *B, int d, mpz_t w);
+
+/* Replaces cu_mpz_rmatrix_mult_fft (src/include/hwmpz.h:132-134,
+   src/lib/hwmpz.c:132-247): the same GPU path (every size, no lgN window). */
+MPZMM_API void cu_mpz_rmatrix_mult_fft(mpz_t *C, mpz_t *A, int r, mpz_t *B, int d, mpz_t w);
+
+/* Replaces mpz_rmatrix_gpu_fft_suitable (src/include/hwmpz.h:136-139,
+   src/lib/hwmpz.c:249-255): 1 if this library can multiply these operands. */
+MPZMM_API int mpz_rmatrix_gpu_fft_suitable(mpz_t *A, int r, mpz_t *B, int d);
+
+/* src/include/hwmpz.h:130 and :134 (header inlines in the reference). */
+static inline void mpz_matrix_mult_fft(mpz_t *C, mpz_t *A, mpz_t *B, int d, mpz_t w) {
+  mpz_rmatrix_mult_fft(C, A, d, B, d, w);
+}
+static inline void cu_mpz_matrix_mult_fft(mpz_t *C, mpz_t *A, mpz_t *B, int d, mpz_t w) {
+  cu_mpz_rmatrix_mult_fft(C, A, d, B, d, w);
+}
+
+/* Fatal-error hook for the void entry points above (default: print the
+   error to stderr and abort()).  No counterpart in the reference. */
+typedef void (*mpzmm_fatal_fn)(int status, const char *message);
+MPZMM_API void mpzmm_set_fatal_hook(mpzmm_fatal_fn fn);
+
+/* ======================================================================
+ * 2. Extended API (no counterpart in the reference)
+ * ====================================================================== */
+
+/* Explicit set-up on a device; returns a status.  hw_mpz_setup() calls it
+   with the default device. */
+MPZMM_API int mpzmm_setup(int device);
+/* Human-readable message for the last error on the calling thread. */
+MPZMM_API const char *mpzmm_last_error(void);
+/* 1 if a CUDA device is usable, else 0 (never aborts). */
+MPZMM_API int mpzmm_device_available(void);
+
+/* Exact C = A * B for A m x k, B k x n, C m x n (packed vectors in host
+   memory).  C entry e is written at c_limbs[c_offs[e]] with capacity
+   c_caps[e] limbs and its signed size stored in c_sizes[e].  A capacity of
+   mpzmm_output_limbs(...) always suffices.  stream: a cudaStream_t, or NULL
+   for the library's own stream.  Synchronous: returns after C is written. */
+MPZMM_API int mpzmm_matmul(int m, int k, int n,
+                 const uint64_t *a_limbs, const int64_t *a_offs, const int32_t *a_sizes,
+                 const uint64_t *b_limbs, const int64_t *b_offs, const int32_t *b_sizes,
+                 uint64_t *c_limbs, const int64_t *c_offs, const int64_t *c_caps,
+                 int32_t *c_sizes, void *stream);
+
+/* Limbs that always suffice for every entry of an m x k by k x n product
+   whose A entries have at most a_bits bits and B entries at most b_bits
+   bits: ceil((a_bits + b_bits + ceil(log2 k) + 1) / 64).  Host-only. */
+MPZMM_API int64_t mpzmm_output_limbs(int k, int64_t a_bits, int64_t b_bits);
+
+/* One product of a batch (host pointers, packed vectors as above). */
+typedef struct mpzmm_product {
+  int m, k, n;
+  const uint64_t *a_limbs;
+  const int64_t *a_offs;
+  const int32_t *a_sizes;
+  const uint64_t *b_limbs;
+  const int64_t *b_offs;
+  const int32_t *b_sizes;
+  uint64_t *c_limbs;
+  const int64_t *c_offs;
+  const int64_t *c_caps;
+  int32_t *c_sizes;
+} mpzmm_product;
+
+/* Many independent products of uneven shapes and sizes in one pass: one
+   launch per pipeline stage for the whole batch.  Synchronous. */
+MPZMM_API int mpzmm_matmul_batch(int count, const mpzmm_product *products, void *stream);
+
+/* ---- device-resident plans (build once, run many times) ---- */
+typedef struct mpzmm_plan mpzmm_plan;
+
+/* Plans a batch and copies its inputs to the device.  The products' host
+   input arrays are only read during this call. */
+MPZMM_API int mpzmm_plan_create(mpzmm_plan **plan, int count, const mpzmm_product *products,
+                      void *stream);
+/* Runs every kernel of the plan on the inputs already resident in device
+   memory; results stay on the device.  Asynchronous on `stream`. */
+MPZMM_API int mpzmm_plan_execute(mpzmm_plan *plan, void *stream);
+/* Copies the results of the last execute into the products' host outputs
+   (c_limbs / c_sizes given at create time).  Synchronous. */
+MPZMM_API int mpzmm_plan_download(mpzmm_plan *plan, void *stream);
+/* Re-reads the products' host inputs into the plan (same shapes and sizes)
+   and copies them to the device.  Asynchronous on `stream`. */
+MPZMM_API int mpzmm_plan_upload(mpzmm_plan *plan, void *stream);
+MPZMM_API void mpzmm_plan_destroy(mpzmm_plan *plan);
+
+/* Stage timing with CUDA events recorded on the execute stream (off by
+   default).  Stages: 0 split + forward NTT, 1 contraction, 2 inverse NTT,
+   3 CRT + recompose.  mpzmm_plan_stage_times waits for the last timed
+   execute, returns the summed milliseconds per stage over all timed
+   executes since the previous call (then resets), the kernel launches per
+   stage of one execute, and how many executes were timed. */
+MPZMM_API int mpzmm_plan_set_timing(mpzmm_plan *plan, int enable);
+MPZMM_API int mpzmm_plan_stage_times(mpzmm_plan *plan, float *ms4, int64_t *launches4,
+                                     int64_t *executes);
+
+/* Statistics of a plan: kernels launched per execute, device bytes, and the
+   chosen (P, r, lgN) of product `index` (any pointer may be NULL). */
+MPZMM_API int mpzmm_plan_info(const mpzmm_plan *plan, int64_t *launches_per_execute,
+                    int64_t *device_bytes, int index, int *P, int *r, int *lgN);
+
+/* Parameters (prime count P, coefficient bits r, transform length 2^lgN)
+   that the planner picks for a product with k terms whose A and B entries
+   have at most a_bits and b_bits bits.  Host-only; no device needed. */
+MPZMM_API int mpzmm_choose_params(int64_t a_bits, int64_t b_bits, int k, int *P, int *r,
+                        int *lgN);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPZMM_B200_H */

@@ -1,0 +1,169 @@
+"""Python front end of libmpzmm_b200 over packed vectors.
+
+Mirrors the reference's operator interface (alexp616/rforest
+src/include/hwmpz.h): ``setup()`` ~ hw_mpz_setup, ``matmul`` ~
+mpz_rmatrix_mult_fft for general m x k by k x n shapes, plus batches and
+device-resident plans.  Every call goes through the C ABI; there is no
+Python or CPU implementation of the product behind it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .packed import Packed
+
+ProductIn = Tuple[int, int, int, Packed, Packed]
+
+
+def _ptr(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+def _stream_arg(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(getattr(stream, "cuda_stream"))  # torch.cuda.Stream
+
+
+def setup(device: int = 0) -> None:
+    _lib.check(_lib.lib().mpzmm_setup(device))
+
+
+def device_available() -> bool:
+    return bool(_lib.lib().mpzmm_device_available())
+
+
+def choose_params(a_bits: int, b_bits: int, k: int) -> Tuple[int, int, int]:
+    P, r, lg = C.c_int(), C.c_int(), C.c_int()
+    _lib.check(_lib.lib().mpzmm_choose_params(a_bits, b_bits, k, C.byref(P), C.byref(r),
+                                              C.byref(lg)))
+    return P.value, r.value, lg.value
+
+
+def output_limbs(k: int, a_bits: int, b_bits: int) -> int:
+    return int(_lib.lib().mpzmm_output_limbs(k, a_bits, b_bits))
+
+
+class _Holder:
+    """Keeps the numpy arrays behind one mpzmm_product alive."""
+
+    def __init__(self, m: int, k: int, n: int, A: Packed, B: Packed):
+        if len(A) != m * k or len(B) != k * n:
+            raise ValueError("entry counts do not match the dimensions")
+        self.m, self.k, self.n = m, k, n
+        self.al = np.ascontiguousarray(A.limbs, dtype=np.uint64)
+        self.bl = np.ascontiguousarray(B.limbs, dtype=np.uint64)
+        if self.al.size == 0:
+            self.al = np.zeros(1, np.uint64)
+        if self.bl.size == 0:
+            self.bl = np.zeros(1, np.uint64)
+        self.ao = np.ascontiguousarray(A.offs, dtype=np.int64)
+        self.bo = np.ascontiguousarray(B.offs, dtype=np.int64)
+        self.asz = np.ascontiguousarray(A.sizes, dtype=np.int32)
+        self.bsz = np.ascontiguousarray(B.sizes, dtype=np.int32)
+        cap = output_limbs(k, 64 * A.max_limbs(), 64 * B.max_limbs())
+        self.caps = np.full(m * n, cap, dtype=np.int64)
+        self.co = np.arange(m * n, dtype=np.int64) * cap
+        self.cl = np.zeros(max(m * n * cap, 1), dtype=np.uint64)
+        self.csz = np.zeros(m * n, dtype=np.int32)
+        self.struct = _lib.Product(
+            m, k, n,
+            _ptr(self.al, _lib.u64p), _ptr(self.ao, _lib.i64p), _ptr(self.asz, _lib.i32p),
+            _ptr(self.bl, _lib.u64p), _ptr(self.bo, _lib.i64p), _ptr(self.bsz, _lib.i32p),
+            _ptr(self.cl, _lib.u64p), _ptr(self.co, _lib.i64p), _ptr(self.caps, _lib.i64p),
+            _ptr(self.csz, _lib.i32p))
+
+    def result(self) -> Packed:
+        return Packed(self.cl, self.co, self.csz)
+
+    def set_inputs(self, A: Packed, B: Packed) -> None:
+        """Overwrite the input limbs in place (same sizes and signs)."""
+        np.copyto(self.al[:A.limbs.size], A.limbs)
+        np.copyto(self.bl[:B.limbs.size], B.limbs)
+
+
+def matmul(m: int, k: int, n: int, A: Packed, B: Packed, stream=None) -> Packed:
+    """Exact C = A * B (A m x k, B k x n, row-major packed vectors)."""
+    h = _Holder(m, k, n, A, B)
+    _lib.check(_lib.lib().mpzmm_matmul_batch(1, C.byref(h.struct), _stream_arg(stream)))
+    return h.result()
+
+
+class Batch:
+    """Host-side arrays of a batch of products, reusable across calls.  Each
+    ``run`` is one full pass through the C ABI (mpzmm_matmul_batch): plan,
+    host->device copy of the inputs, all kernels, device->host copy of the
+    results into the host output arrays."""
+
+    def __init__(self, products: Sequence[ProductIn]):
+        self.holders = [_Holder(*p) for p in products]
+        self.arr = (_lib.Product * len(self.holders))(*[h.struct for h in self.holders])
+
+    def run(self, stream=None) -> List[Packed]:
+        _lib.check(_lib.lib().mpzmm_matmul_batch(len(self.holders), self.arr,
+                                                 _stream_arg(stream)))
+        return [h.result() for h in self.holders]
+
+
+def matmul_batch(products: Sequence[ProductIn], stream=None) -> List[Packed]:
+    """Many independent products in one pass (one launch per stage)."""
+    return Batch(products).run(stream)
+
+
+class Plan:
+    """A device-resident batch: inputs uploaded once, executed many times."""
+
+    def __init__(self, products: Sequence[ProductIn], stream=None):
+        self.holders = [_Holder(*p) for p in products]
+        self.arr = (_lib.Product * len(self.holders))(*[h.struct for h in self.holders])
+        self.handle = C.c_void_p()
+        _lib.check(_lib.lib().mpzmm_plan_create(C.byref(self.handle), len(self.holders),
+                                                self.arr, _stream_arg(stream)))
+
+    def execute(self, stream=None) -> None:
+        _lib.check(_lib.lib().mpzmm_plan_execute(self.handle, _stream_arg(stream)))
+
+    def upload(self, stream=None) -> None:
+        _lib.check(_lib.lib().mpzmm_plan_upload(self.handle, _stream_arg(stream)))
+
+    def download(self, stream=None) -> List[Packed]:
+        _lib.check(_lib.lib().mpzmm_plan_download(self.handle, _stream_arg(stream)))
+        return [h.result() for h in self.holders]
+
+    def info(self, index: int = 0):
+        launches, nbytes = C.c_int64(), C.c_int64()
+        P, r, lg = C.c_int(), C.c_int(), C.c_int()
+        _lib.check(_lib.lib().mpzmm_plan_info(self.handle, C.byref(launches), C.byref(nbytes),
+                                              index, C.byref(P), C.byref(r), C.byref(lg)))
+        return {"launches": launches.value, "device_bytes": nbytes.value,
+                "P": P.value, "r": r.value, "lgN": lg.value}
+
+    def set_timing(self, on: bool) -> None:
+        _lib.check(_lib.lib().mpzmm_plan_set_timing(self.handle, 1 if on else 0))
+
+    def stage_times(self):
+        """(ms per stage summed over timed executes, launches per stage per
+        execute, timed executes); stages: fwd, contract, inv, crt."""
+        ms = (C.c_float * 4)()
+        launches = (C.c_int64 * 4)()
+        ex = C.c_int64()
+        _lib.check(_lib.lib().mpzmm_plan_stage_times(
+            self.handle, ms, C.cast(launches, _lib.i64p), C.byref(ex)))
+        return list(ms), list(launches), ex.value
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.lib().mpzmm_plan_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

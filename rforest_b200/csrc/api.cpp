@@ -1,0 +1,250 @@
+// extern "C" entry points of libmpzmm_b200.so (declared in include/mpzmm_b200.h).
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "../../include/mpzmm_b200.h"
+#include "engine.h"
+
+using namespace mpzmm;
+
+namespace {
+
+void default_fatal(int status, const char* msg) {
+  std::fprintf(stderr, "mpzmm_b200: fatal error %d: %s\n", status, msg);
+  std::abort();
+}
+mpzmm_fatal_fn g_fatal = default_fatal;
+std::mutex g_call_mu;  // the reference API is single-threaded global state
+
+cudaStream_t pick_stream(void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : context().stream;
+}
+
+int build_spec_packed(const mpzmm_product& p, ProductSpec* ps) {
+  if (p.m < 0 || p.k < 0 || p.n < 0) return set_error(kErrArg, "negative dimension");
+  ps->m = p.m;
+  ps->k = p.k;
+  ps->n = p.n;
+  const int64_t na = (int64_t)p.m * p.k, nb = (int64_t)p.k * p.n, nc = (int64_t)p.m * p.n;
+  if ((na && (!p.a_offs || !p.a_sizes)) || (nb && (!p.b_offs || !p.b_sizes)) ||
+      (nc && (!p.c_offs || !p.c_caps || !p.c_sizes || !p.c_limbs)))
+    return set_error(kErrArg, "null array");
+  ps->a.resize(na);
+  ps->b.resize(nb);
+  ps->c.resize(nc);
+  for (int64_t e = 0; e < na; ++e) {
+    const int32_t s = p.a_sizes[e];
+    ps->a[e] = EntryRef{s ? p.a_limbs + p.a_offs[e] : nullptr, s};
+  }
+  for (int64_t e = 0; e < nb; ++e) {
+    const int32_t s = p.b_sizes[e];
+    ps->b[e] = EntryRef{s ? p.b_limbs + p.b_offs[e] : nullptr, s};
+  }
+  for (int64_t e = 0; e < nc; ++e)
+    ps->c[e] = OutRef{p.c_limbs + p.c_offs[e], p.c_caps[e], p.c_sizes + e, nullptr};
+  return kOk;
+}
+
+int run_once(std::vector<ProductSpec> specs, void* stream) {
+  int st = ensure_setup(-1);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(workspace_mutex());
+  Plan plan;
+  if ((st = plan.build(std::move(specs), context().ws))) return st;
+  cudaStream_t s = pick_stream(stream);
+  if ((st = plan.upload(s))) return st;
+  if ((st = plan.execute(s))) return st;
+  return plan.download(s);
+}
+
+// r x d by d x d over mpz_t arrays (src/lib/hwmpz.c:65-130)
+int mpz_matmul(mpz_t* C, mpz_t* A, int r, mpz_t* B, int d) {
+  if (r < 0 || d < 0) return set_error(kErrArg, "negative dimension");
+  ProductSpec ps;
+  ps.m = r;
+  ps.k = d;
+  ps.n = d;
+  ps.a.resize((size_t)r * d);
+  ps.b.resize((size_t)d * d);
+  ps.c.resize((size_t)r * d);
+  for (size_t e = 0; e < ps.a.size(); ++e)
+    ps.a[e] = EntryRef{reinterpret_cast<const uint64_t*>(A[e]->_mp_d), A[e]->_mp_size};
+  for (size_t e = 0; e < ps.b.size(); ++e)
+    ps.b[e] = EntryRef{reinterpret_cast<const uint64_t*>(B[e]->_mp_d), B[e]->_mp_size};
+  for (size_t e = 0; e < ps.c.size(); ++e) ps.c[e] = OutRef{nullptr, 0, nullptr, C[e]};
+  std::vector<ProductSpec> v;
+  v.push_back(std::move(ps));
+  return run_once(std::move(v), nullptr);
+}
+
+}  // namespace
+
+struct mpzmm_plan {
+  Plan plan;
+};
+
+extern "C" {
+
+void mpzmm_set_fatal_hook(mpzmm_fatal_fn fn) { g_fatal = fn ? fn : default_fatal; }
+
+int mpzmm_setup(int device) { return ensure_setup(device); }
+
+const char* mpzmm_last_error(void) { return last_error(); }
+
+int mpzmm_device_available(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n > 0 ? 1 : 0;
+}
+
+void hw_mpz_setup(void) {
+  std::lock_guard<std::mutex> lk(g_call_mu);
+  int st = ensure_setup(-1);
+  if (st) g_fatal(st, last_error());
+}
+
+void hw_mpz_clear(void) {
+  std::lock_guard<std::mutex> lk(g_call_mu);
+  teardown();
+}
+
+void mpz_rmatrix_mult_fft(mpz_t* C, mpz_t* A, int r, mpz_t* B, int d, mpz_t w) {
+  (void)w;
+  std::lock_guard<std::mutex> lk(g_call_mu);
+  if (!context().ready) {
+    g_fatal(kErrState, "mpz_rmatrix_mult_fft called before hw_mpz_setup");
+    return;
+  }
+  int st = mpz_matmul(C, A, r, B, d);
+  if (st) g_fatal(st, last_error());
+}
+
+void cu_mpz_rmatrix_mult_fft(mpz_t* C, mpz_t* A, int r, mpz_t* B, int d, mpz_t w) {
+  mpz_rmatrix_mult_fft(C, A, r, B, d, w);
+}
+
+int mpz_rmatrix_gpu_fft_suitable(mpz_t* A, int r, mpz_t* B, int d) {
+  if (r < 0 || d < 0) return 0;
+  int64_t ab = 0, bb = 0;
+  for (int64_t e = 0; e < (int64_t)r * d; ++e) {
+    int64_t s = A[e]->_mp_size < 0 ? -(int64_t)A[e]->_mp_size : A[e]->_mp_size;
+    if (64 * s > ab) ab = 64 * s;
+  }
+  for (int64_t e = 0; e < (int64_t)d * d; ++e) {
+    int64_t s = B[e]->_mp_size < 0 ? -(int64_t)B[e]->_mp_size : B[e]->_mp_size;
+    if (64 * s > bb) bb = 64 * s;
+  }
+  Params prm;
+  return choose_params(ab, bb, r, d, d, &prm) ? 1 : 0;
+}
+
+int64_t mpzmm_output_limbs(int k, int64_t a_bits, int64_t b_bits) {
+  return output_limbs(k, a_bits, b_bits);
+}
+
+int mpzmm_choose_params(int64_t a_bits, int64_t b_bits, int k, int* P, int* r, int* lgN) {
+  Params prm;
+  if (!choose_params(a_bits, b_bits, 1, k, 1, &prm))
+    return set_error(kErrTooLarge, "no supported parameters");
+  if (P) *P = prm.P;
+  if (r) *r = prm.r;
+  if (lgN) *lgN = prm.lgN;
+  return kOk;
+}
+
+int mpzmm_matmul(int m, int k, int n, const uint64_t* a_limbs, const int64_t* a_offs,
+                 const int32_t* a_sizes, const uint64_t* b_limbs, const int64_t* b_offs,
+                 const int32_t* b_sizes, uint64_t* c_limbs, const int64_t* c_offs,
+                 const int64_t* c_caps, int32_t* c_sizes, void* stream) {
+  mpzmm_product p{m,      k,      n,       a_limbs, a_offs, a_sizes, b_limbs,
+                  b_offs, b_sizes, c_limbs, c_offs,  c_caps, c_sizes};
+  return mpzmm_matmul_batch(1, &p, stream);
+}
+
+int mpzmm_matmul_batch(int count, const mpzmm_product* products, void* stream) {
+  if (count < 0 || (count > 0 && !products)) return set_error(kErrArg, "bad product list");
+  std::vector<ProductSpec> specs((size_t)count);
+  for (int t = 0; t < count; ++t) {
+    int st = build_spec_packed(products[t], &specs[t]);
+    if (st) return st;
+  }
+  return run_once(std::move(specs), stream);
+}
+
+int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* products,
+                      void* stream) {
+  if (!plan) return set_error(kErrArg, "null plan pointer");
+  *plan = nullptr;
+  if (count < 0 || (count > 0 && !products)) return set_error(kErrArg, "bad product list");
+  int st = ensure_setup(-1);
+  if (st) return st;
+  std::vector<ProductSpec> specs((size_t)count);
+  for (int t = 0; t < count; ++t) {
+    if ((st = build_spec_packed(products[t], &specs[t]))) return st;
+  }
+  std::unique_ptr<mpzmm_plan> p(new mpzmm_plan);
+  if ((st = p->plan.build(std::move(specs)))) return st;
+  if ((st = p->plan.upload(pick_stream(stream)))) return st;
+  *plan = p.release();
+  return kOk;
+}
+
+int mpzmm_plan_execute(mpzmm_plan* plan, void* stream) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  return plan->plan.execute(pick_stream(stream));
+}
+
+int mpzmm_plan_download(mpzmm_plan* plan, void* stream) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  return plan->plan.download(pick_stream(stream));
+}
+
+int mpzmm_plan_upload(mpzmm_plan* plan, void* stream) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  return plan->plan.upload(pick_stream(stream));
+}
+
+void mpzmm_plan_destroy(mpzmm_plan* plan) { delete plan; }
+
+int mpzmm_plan_set_timing(mpzmm_plan* plan, int enable) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  plan->plan.set_timing(enable != 0);
+  return kOk;
+}
+
+int mpzmm_plan_stage_times(mpzmm_plan* plan, float* ms, int64_t* launches,
+                           int64_t* executes) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  float t[Plan::kStages];
+  int st = plan->plan.stage_times(t, executes);
+  if (st) return st;
+  int64_t l[Plan::kStages];
+  plan->plan.stage_launches(l);
+  for (int s = 0; s < Plan::kStages; ++s) {
+    if (ms) ms[s] = t[s];
+    if (launches) launches[s] = l[s];
+  }
+  return kOk;
+}
+
+int mpzmm_plan_info(const mpzmm_plan* plan, int64_t* launches, int64_t* bytes, int index,
+                    int* P, int* r, int* lgN) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  if (launches) *launches = plan->plan.launches_per_execute();
+  if (bytes) *bytes = plan->plan.device_bytes();
+  const auto& prm = plan->plan.params();
+  if (index >= 0 && index < (int)prm.size()) {
+    if (P) *P = prm[index].P;
+    if (r) *r = prm[index].r;
+    if (lgN) *lgN = prm[index].lgN;
+  }
+  return kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+// Batch engine: plans a set of independent products, moves their limbs to
+// the device, runs the four pipeline stages with one launch per stage and
+// size class, and brings the results back.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "mpzmm_internal.h"
+#include "planner.h"
+
+namespace mpzmm {
+
+// Status codes (same values as the public header).
+enum Status : int {
+  kOk = 0,
+  kErrArg = 1,
+  kErrTooLarge = 2,
+  kErrCapacity = 3,
+  kErrCuda = 4,
+  kErrNoMem = 5,
+  kErrState = 6,
+  kErrTimeout = 7,
+  kErrBusy = 8,
+};
+
+int set_error(int status, const std::string& msg);
+const char* last_error();
+
+// One integer operand: limb pointer and GMP-style signed size.
+struct EntryRef {
+  const uint64_t* d;
+  int32_t size;
+};
+
+// Where one output entry goes.
+struct OutRef {
+  uint64_t* d;       // destination limbs (packed output) or nullptr (mpz)
+  int64_t cap;       // capacity in limbs (packed output)
+  int32_t* size;     // signed size destination (packed output)
+  void* mpz;         // mpz_ptr destination (mpz output) or nullptr
+};
+
+struct ProductSpec {
+  int m = 0, k = 0, n = 0;
+  std::vector<EntryRef> a, b;  // m*k and k*n entries, row-major
+  std::vector<OutRef> c;       // m*n entries
+};
+
+// Device and pinned host buffers of a plan.  Grow-only, so one workspace is
+// reused by every one-shot call (no per-call cudaMalloc / cudaMallocHost once
+// it has reached the working size).
+struct Workspace {
+  uint64_t* d_limbs = nullptr;
+  uint32_t* d_res = nullptr;
+  uint32_t* d_out = nullptr;
+  int32_t* d_sizes = nullptr;
+  uint8_t* d_desc = nullptr;
+  uint64_t* h_limbs = nullptr;
+  uint32_t* h_out = nullptr;
+  int32_t* h_sizes = nullptr;
+  uint8_t* h_desc = nullptr;
+  size_t cap_limbs = 0, cap_res = 0, cap_out = 0, cap_sizes = 0, cap_desc = 0;
+  size_t hcap_limbs = 0, hcap_out = 0, hcap_sizes = 0, hcap_desc = 0;
+  int64_t device_bytes = 0;
+  // Ensures room for the given element counts; returns a status.
+  int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes);
+  void release();
+  ~Workspace() { release(); }
+};
+
+// Process-wide device state: tables on the device, default stream.
+struct Context {
+  bool ready = false;
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  uint2* d_twf = nullptr;
+  uint2* d_twi = nullptr;
+  int num_sms = 0;
+  Workspace* ws = nullptr;  // shared by one-shot calls (guarded by ws_mu)
+};
+
+Context& context();
+std::mutex& workspace_mutex();
+
+// Runs fn(lo, hi) over [0, n) split across host threads when `bytes` is
+// large enough to be worth it (gather/scatter of limbs).
+void parallel_chunks(size_t n, size_t bytes, const std::function<void(size_t, size_t)>& fn);
+int ensure_setup(int device);
+void teardown();
+
+class Plan {
+ public:
+  static constexpr int kStages = 4;
+  ~Plan();
+  // Computes parameters, descriptors and launch groups, and reserves device
+  // and pinned host buffers in `ws` (the plan's own workspace if null).
+  int build(std::vector<ProductSpec> prods, Workspace* ws = nullptr);
+  // Gathers input limbs into pinned memory and copies them (and the
+  // descriptors) to the device.
+  int upload(cudaStream_t st);
+  // Runs split+fwd NTT, contraction, inverse NTT, CRT+recompose.
+  int execute(cudaStream_t st);
+  // Copies outputs back and writes them to the output references.
+  int download(cudaStream_t st);
+
+  int64_t launches_per_execute() const { return launches_; }
+  // Stage timing with CUDA events recorded on the execute stream: stages are
+  // 0 split+forward NTT, 1 contraction, 2 inverse NTT, 3 CRT+recompose.
+  void set_timing(bool on) { timing_ = on; }
+  int stage_times(float ms[kStages], int64_t* executes);
+  void stage_launches(int64_t out[kStages]) const;
+  int64_t device_bytes() const { return ws_ ? ws_->device_bytes : 0; }
+  const std::vector<Params>& params() const { return params_; }
+  std::vector<ProductSpec>& products() { return prods_; }
+
+ private:
+  struct Group {
+    int P = 0, lgN = 0;
+    uint32_t idx_off = 0;  // into the device index array
+    std::vector<uint32_t> idx;
+    int words_per_thread = 1;
+    size_t smem = 0;
+  };
+
+  std::vector<ProductSpec> prods_;
+  std::vector<Params> params_;
+  std::vector<FwdDesc> fwd_;
+  std::vector<InvDesc> inv_;
+  std::vector<ProdDesc> pd_;
+  std::vector<ContractItem> items_;
+  std::vector<Group> fwd_groups_, inv_groups_, rec_groups_;
+  std::vector<uint32_t> idx_all_;
+  std::vector<OutRef> outs_;          // flattened output references
+  std::vector<int64_t> out_word_off_; // per output entry (words)
+  std::vector<uint8_t> zero_prod_;    // product is identically zero
+
+  uint64_t n_limbs_ = 0, n_res_ = 0, n_out_words_ = 0;
+  int64_t launches_ = 0;
+
+  Workspace own_;
+  Workspace* ws_ = nullptr;
+  // descriptor blob: offsets of each section (bytes) and its size
+  size_t off_fwd_ = 0, off_inv_ = 0, off_pd_ = 0, off_items_ = 0, off_idx_ = 0, desc_bytes_ = 0;
+  FwdDesc* d_fwd_ = nullptr;
+  InvDesc* d_inv_ = nullptr;
+  ProdDesc* d_pd_ = nullptr;
+  ContractItem* d_items_ = nullptr;
+  uint32_t* d_idx_ = nullptr;
+  bool built_ = false;
+  bool timing_ = false;
+  std::vector<cudaEvent_t> events_;  // kStages + 1 per timed execute
+};
+
+}  // namespace mpzmm

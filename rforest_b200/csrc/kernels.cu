@@ -1,0 +1,581 @@
+// sm_100a kernels of the exact matrix-product pipeline.
+//
+//   k_split_fwd      limbs -> r-bit coefficients -> residues mod p -> forward
+//                    NTT in shared memory (one CTA per (entry, prime))
+//   k_contract       per frequency h and prime: C[h] = A[h] B[h] mod p on
+//                    CUDA cores (64-bit lazy accumulation, Montgomery fold)
+//   k_inv_ntt        inverse NTT in shared memory (one CTA per (entry, prime))
+//   k_crt_recompose  Garner CRT to signed multi-word coefficients, then
+//                    sum_i c_i 2^(i r) as a carry-lookahead prefix scan over
+//                    32-bit output words, sign + negation + normalisation
+//                    (one CTA per output entry)
+//
+// Reference counterparts: split/reduce src/lib/split_reduce.c:15-66,
+// NTTs src/lib/mpnfft.c:354-432, contraction src/lib/mpnfft.c:559-651,
+// CRT src/lib/crt.c:11-94, recompose src/lib/recompose.c:11-107 and
+// src/lib/crt_recompose.c:15-156, sign/normalise src/lib/hwmpz.c:116-122.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+#include "modarith.cuh"
+#include "mpzmm_internal.h"
+
+namespace mpzmm {
+
+__constant__ PrimeConst c_primes[kMaxPrimes];
+__constant__ CrtConst c_crt;
+
+constexpr int kTwStride = 1 << kTwiddleLg;  // twiddle entries per prime
+
+// ---------------------------------------------------------------------------
+// NTT building blocks (shared memory, radix-2)
+//
+// Forward (Cooley-Tukey, natural order in, bit-reversed order out): for
+// m = 1, 2, ..., N/2 and t = N/(2m), block i of 2t values is split with the
+// twiddle T[m + i] = w_{2m}^{brev(i)}, a primitive-root power that does not
+// depend on N, so one table of 2^kTwiddleLg entries per prime serves every N.
+// Inverse (Gentleman-Sande) runs the same (m, i) pairs in reverse order with
+// T^{-1}; it returns N times the input, the factor is removed before CRT.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ntt_fwd_smem(uint32_t* a, int lgN, const uint2* tw,
+                                             uint32_t p) {
+  const int half = 1 << (lgN - 1);
+  for (int lgm = 0; lgm < lgN; ++lgm) {
+    const int lgt = lgN - 1 - lgm;
+    const int t = 1 << lgt;
+    const int m = 1 << lgm;
+    for (int b = threadIdx.x; b < half; b += blockDim.x) {
+      const int i = b >> lgt;
+      const int j = (i << (lgt + 1)) + (b & (t - 1));
+      const uint2 S = tw[m + i];
+      const uint32_t U = a[j];
+      const uint32_t V = mul_shoup(a[j + t], S.x, S.y, p);
+      a[j] = add_mod(U, V, p);
+      a[j + t] = sub_mod(U, V, p);
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void ntt_inv_smem(uint32_t* a, int lgN, const uint2* tw,
+                                             uint32_t p) {
+  const int half = 1 << (lgN - 1);
+  for (int lgm = lgN - 1; lgm >= 0; --lgm) {
+    const int lgt = lgN - 1 - lgm;
+    const int t = 1 << lgt;
+    const int m = 1 << lgm;
+    for (int b = threadIdx.x; b < half; b += blockDim.x) {
+      const int i = b >> lgt;
+      const int j = (i << (lgt + 1)) + (b & (t - 1));
+      const uint2 S = tw[m + i];
+      const uint32_t X = a[j];
+      const uint32_t Y = a[j + t];
+      a[j] = add_mod(X, Y, p);
+      a[j + t] = mul_shoup(sub_mod(X, Y, p), S.x, S.y, p);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Split + reduce + forward NTT.  grid = (entries of this class, P).
+// Coefficient i of an entry is bits [i r, (i+1) r) of its magnitude; its
+// residue is taken by Horner over 32-bit words (Shoup multiply by 2^32 mod p)
+// and negated for a negative entry, which is how the reference folds the
+// sign into the split (src/lib/split_reduce.c:27-38).
+// ---------------------------------------------------------------------------
+__global__ void k_split_fwd(const FwdDesc* __restrict__ descs,
+                            const uint32_t* __restrict__ idx,
+                            const uint64_t* __restrict__ limbs,
+                            uint32_t* __restrict__ res,
+                            const uint2* __restrict__ twf) {
+  extern __shared__ uint32_t sm[];
+  const FwdDesc d = descs[idx[blockIdx.x]];
+  const int j = blockIdx.y;
+  const uint32_t p = c_primes[j].p;
+  const uint32_t mu = c_primes[j].mu;
+  const uint32_t b32 = c_primes[j].b32;
+  const uint32_t b32q = c_primes[j].b32q;
+  const int N = 1 << d.lgN;
+  const uint32_t nl = (uint32_t)(d.size < 0 ? -d.size : d.size);
+  const uint32_t nw = 2 * nl;
+  const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
+  const uint32_t r = d.r;
+  const int ncw = (int)((r + 31) >> 5);
+  const uint32_t topbits = r - 32u * (uint32_t)(ncw - 1);
+  const uint32_t topmask = topbits >= 32 ? 0xffffffffu : ((1u << topbits) - 1u);
+  const bool neg = d.size < 0;
+
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    uint32_t v = 0;
+    if ((uint32_t)i < d.ncoef) {
+      const uint64_t bit = (uint64_t)i * r;
+      const uint64_t wi = bit >> 5;
+      const uint32_t sh = (uint32_t)(bit & 31);
+      uint32_t acc = 0;
+      for (int q = ncw - 1; q >= 0; --q) {
+        const uint64_t a0 = wi + (uint64_t)q;
+        const uint32_t lo = a0 < nw ? w32[a0] : 0u;
+        const uint32_t hi = a0 + 1 < nw ? w32[a0 + 1] : 0u;
+        uint32_t c = __funnelshift_r(lo, hi, sh);
+        if (q == ncw - 1) c &= topmask;
+        acc = add_mod(mul_shoup(acc, b32, b32q, p), mod32(c, p, mu), p);
+      }
+      v = (neg && acc) ? p - acc : acc;
+    }
+    sm[i] = v;
+  }
+  __syncthreads();
+  ntt_fwd_smem(sm, d.lgN, twf + (size_t)j * kTwStride, p);
+  uint32_t* out = res + d.res_off + (uint64_t)j * (uint64_t)N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) out[i] = sm[i];
+}
+
+// ---------------------------------------------------------------------------
+// Inverse NTT.  grid = (entries of this class, P).
+// ---------------------------------------------------------------------------
+__global__ void k_inv_ntt(const InvDesc* __restrict__ descs,
+                          const uint32_t* __restrict__ idx, uint32_t* __restrict__ res,
+                          const uint2* __restrict__ twi) {
+  extern __shared__ uint32_t sm[];
+  const InvDesc d = descs[idx[blockIdx.x]];
+  const int j = blockIdx.y;
+  const uint32_t p = c_primes[j].p;
+  const int N = 1 << d.lgN;
+  uint32_t* io = res + d.res_off + (uint64_t)j * (uint64_t)N;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sm[i] = io[i];
+  __syncthreads();
+  ntt_inv_smem(sm, d.lgN, twi + (size_t)j * kTwStride, p);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) io[i] = sm[i];
+}
+
+// ---------------------------------------------------------------------------
+// Contraction on CUDA cores.  One thread per frequency h; it walks the m x n
+// outputs in strips of 4 columns.  Products of residues < p < 2^30 are < 2^60,
+// so sixteen of them accumulate exactly in 64 bits before a Montgomery fold
+// (the reference reduces every 16 terms for the same reason with 128-bit
+// accumulators, src/lib/mpnfft.c:621-627).  Outputs carry a factor 2^-32
+// that the CRT stage removes.
+// ---------------------------------------------------------------------------
+constexpr int kContractThreads = 128;
+
+__global__ void __launch_bounds__(kContractThreads)
+k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
+           uint32_t* __restrict__ res) {
+  const ContractItem it = items[blockIdx.x];
+  const ProdDesc d = prods[it.prod];
+  const int N = 1 << d.lgN;
+  const uint32_t h = it.h0 + threadIdx.x;
+  if (h >= (uint32_t)N) return;
+  const int j = it.prime;
+  const uint32_t p = c_primes[j].p;
+  const uint32_t pinv = c_primes[j].pinv;
+  const uint32_t mu = c_primes[j].mu;
+  const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
+  const uint64_t base = (uint64_t)j * (uint64_t)N + h;
+  const uint32_t* __restrict__ A = res + d.a_res + base;
+  const uint32_t* __restrict__ B = res + d.b_res + base;
+  uint32_t* C = res + d.c_res + base;
+  const int m = d.m, k = d.k, n = d.n;
+  for (int i = 0; i < m; ++i) {
+    const uint32_t* Arow = A + (uint64_t)(i * k) * stride;
+    for (int l0 = 0; l0 < n; l0 += 4) {
+      const int nc = (n - l0) < 4 ? (n - l0) : 4;
+      uint64_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+      uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+      int cnt = 0;
+      for (int kk = 0; kk < k; ++kk) {
+        const uint32_t a = __ldg(Arow + (uint64_t)kk * stride);
+        const uint32_t* Bk = B + (uint64_t)(kk * n + l0) * stride;
+        acc0 += (uint64_t)a * __ldg(Bk);
+        if (nc > 1) acc1 += (uint64_t)a * __ldg(Bk + stride);
+        if (nc > 2) acc2 += (uint64_t)a * __ldg(Bk + 2 * stride);
+        if (nc > 3) acc3 += (uint64_t)a * __ldg(Bk + 3 * stride);
+        if (++cnt == 16) {
+          s0 = add_mod(s0, redc64(acc0, p, pinv, mu), p);
+          s1 = add_mod(s1, redc64(acc1, p, pinv, mu), p);
+          s2 = add_mod(s2, redc64(acc2, p, pinv, mu), p);
+          s3 = add_mod(s3, redc64(acc3, p, pinv, mu), p);
+          acc0 = acc1 = acc2 = acc3 = 0;
+          cnt = 0;
+        }
+      }
+      if (cnt) {
+        s0 = add_mod(s0, redc64(acc0, p, pinv, mu), p);
+        s1 = add_mod(s1, redc64(acc1, p, pinv, mu), p);
+        s2 = add_mod(s2, redc64(acc2, p, pinv, mu), p);
+        s3 = add_mod(s3, redc64(acc3, p, pinv, mu), p);
+      }
+      uint32_t* Cr = C + (uint64_t)(i * n + l0) * stride;
+      Cr[0] = s0;
+      if (nc > 1) Cr[stride] = s1;
+      if (nc > 2) Cr[2 * stride] = s2;
+      if (nc > 3) Cr[3 * stride] = s3;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CRT + recompose + sign + normalise.  One CTA per output entry.
+//
+// Coefficient i of the entry is recovered by Garner's algorithm as the
+// symmetric residue X_i in (-M/2, M/2], M = p_0...p_{P-1}, and written as
+// X_i = U_i - s_i 2^(32P) with U_i the P-word two's complement and s_i its
+// sign bit.  The entry is sum_i X_i 2^(i r) mod 2^(32 W).  Output word w
+// gathers its local sum
+//      s_w = sum_i slice_w(U_i 2^(i r)) - sum_i s_i [borrow of i lands in w]
+// (a small signed 64-bit value), then s_w = lo_w + 2^32 hi_w is rewritten as
+// words y_w with carries g_w in {-1,0,1}; the remaining carry ripple is a
+// prefix scan whose element is the word's transfer function
+// {-1,0,1} -> {-1,0,1}, composed associatively.  This is the parallel form
+// of the reference's serial borrow chain (src/lib/recompose.c:43-87) and of
+// its chunk fix-up (src/lib/crt_recompose.c:101-153).
+// ---------------------------------------------------------------------------
+constexpr int kRecThreads = 256;
+
+__device__ __forceinline__ int apply_tf(uint32_t f, int c) {
+  return (int)((f >> (2 * (c + 1))) & 3u) - 1;
+}
+// g after f
+__device__ __forceinline__ uint32_t compose_tf(uint32_t g, uint32_t f) {
+  uint32_t out = 0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const uint32_t fc = (f >> (2 * c)) & 3u;
+    out |= ((g >> (2 * fc)) & 3u) << (2 * c);
+  }
+  return out;
+}
+constexpr uint32_t kTfIdentity = (0u) | (1u << 2) | (2u << 4);
+
+__device__ __forceinline__ uint32_t word_tf(uint32_t y, int g) {
+  uint32_t f = 0;
+#pragma unroll
+  for (int c = -1; c <= 1; ++c) {
+    int delta = 0;
+    if (c == 1 && y == 0xffffffffu) delta = 1;
+    if (c == -1 && y == 0u) delta = -1;
+    f |= (uint32_t)(g + delta + 1) << (2 * (c + 1));
+  }
+  return f;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kRecThreads)
+k_crt_recompose(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
+                const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
+                int32_t* __restrict__ out_sizes, int words_per_thread) {
+  extern __shared__ uint32_t sm[];
+  __shared__ uint32_t s_post[P], s_postq[P];
+  __shared__ uint32_t s_warp_tf[kRecThreads / 32];
+  __shared__ int s_warp_hi[kRecThreads / 32];
+  __shared__ int s_hi_prev, s_carry;
+  __shared__ uint32_t s_top;
+  __shared__ int s_first_nz, s_last_nz, s_last_no;
+
+  const InvDesc d = descs[idx[blockIdx.x]];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int bs = blockDim.x;
+  const int N = 1 << d.lgN;
+  const int64_t r = d.r;
+  const int64_t W = d.out_words;
+  const int64_t ncoef = d.ncoef;
+  uint32_t* o = out + d.out_word;
+  const int64_t TW = (int64_t)bs * words_per_thread;
+
+  if (tid < P) {
+    const uint32_t p = c_primes[tid].p;
+    // N^{-1} mod p = p - (p-1)/N since p = 1 mod N; the contraction left a
+    // Montgomery factor 2^-32, so scale by 2^32 N^{-1} = redc(2^64 N^{-1}).
+    const uint32_t ninv = p - ((p - 1) >> d.lgN);
+    const uint32_t post = redc((uint64_t)c_primes[tid].r2 * ninv, p, c_primes[tid].pinv);
+    s_post[tid] = post;
+    s_postq[tid] = shoup_of(post, p);
+  }
+  if (tid == 0) {
+    s_hi_prev = 0;
+    s_carry = 0;
+    s_top = 0;
+    s_first_nz = 0x7fffffff;
+    s_last_nz = -1;
+    s_last_no = -1;
+  }
+  __syncthreads();
+
+  uint32_t* sU = sm;  // [cmax][P] words, then sign bytes
+  int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
+
+  for (int64_t w0 = 0; w0 < W; w0 += TW) {
+    // coefficients overlapping words [w0, w0 + TW), borrow landings included
+    int64_t lo_i = (32 * w0 - 32 * (int64_t)P + r - 1) / r;  // ceil, may be < 0
+    if (32 * w0 - 32 * (int64_t)P < 0) lo_i = 0;
+    int64_t hi_i = (32 * (w0 + TW) - 1) / r;
+    if (hi_i > ncoef - 1) hi_i = ncoef - 1;
+    const int64_t ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
+    uint8_t* sS = reinterpret_cast<uint8_t*>(sU + (size_t)ncf * P);
+
+    // ---- Garner for every coefficient of the tile ----
+    for (int64_t c = tid; c < ncf; c += bs) {
+      const int64_t ic = lo_i + c;
+      uint32_t v[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const uint32_t p = c_primes[q].p;
+        uint32_t x = res[d.res_off + (uint64_t)q * N + ic];
+        x = mul_shoup(x, s_post[q], s_postq[q], p);
+        if (q == 0) {
+          v[0] = x;
+        } else {
+          // t = (v_0 + v_1 p_0 + ... + v_{q-1} p_0...p_{q-2}) mod p_q (Horner)
+          uint32_t t = v[q - 1] >= p ? v[q - 1] - p : v[q - 1];
+#pragma unroll
+          for (int a = q - 2; a >= 0; --a) {
+            uint32_t va = v[a] >= p ? v[a] - p : v[a];
+            t = add_mod(mul_shoup(t, c_crt.pmod[q][a], c_crt.pmodq[q][a], p), va, p);
+          }
+          v[q] = mul_shoup(sub_mod(x, t, p), c_crt.inv[q], c_crt.invq[q], p);
+        }
+      }
+      // X = v_{P-1}; X = X p_i + v_i for i = P-2 .. 0
+      uint32_t X[P];
+#pragma unroll
+      for (int q = 0; q < P; ++q) X[q] = 0;
+      X[0] = v[P - 1];
+#pragma unroll
+      for (int i = P - 2; i >= 0; --i) {
+        const uint32_t pi = c_primes[i].p;
+        uint64_t cy = v[i];
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const uint64_t t = (uint64_t)X[q] * pi + cy;
+          X[q] = (uint32_t)t;
+          cy = t >> 32;
+        }
+      }
+      // symmetric residue: X > M/2  ->  X - M (two's complement, P words)
+      bool gt = false, decided = false;
+#pragma unroll
+      for (int q = P - 1; q >= 0; --q) {
+        const uint32_t hq = c_crt.Mhalf[P][q];
+        if (!decided && X[q] != hq) {
+          gt = X[q] > hq;
+          decided = true;
+        }
+      }
+      if (gt) {
+        uint32_t br = 0;
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const uint64_t t = (uint64_t)X[q] - c_crt.M[P][q] - br;
+          X[q] = (uint32_t)t;
+          br = (uint32_t)(t >> 63);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < P; ++q) sU[c * P + q] = X[q];
+      sS[c] = gt ? 1 : 0;
+    }
+    __syncthreads();
+
+    // ---- word sums, carry normalisation and the carry scan ----
+    for (int s = 0; s < words_per_thread; ++s) {
+      const int64_t w = w0 + (int64_t)s * bs + tid;
+      const bool active = w < W && w < w0 + TW;
+      int64_t sw = 0;
+      if (active) {
+        int64_t ia = (32 * w - 32 * (int64_t)P + r - 1) / r;
+        if (32 * w - 32 * (int64_t)P < 0) ia = 0;
+        if (ia < lo_i) ia = lo_i;
+        int64_t ib = (32 * w + 31) / r;
+        if (ib > hi_i) ib = hi_i;
+        for (int64_t i = ia; i <= ib; ++i) {
+          const int64_t c = i - lo_i;
+          const int64_t bi = i * r;
+          const int64_t dd = 32 * w - bi;  // bit of U_i that lands on bit 0 of w
+          const uint32_t* U = sU + c * P;
+          uint32_t slice;
+          if (dd < 0) {
+            slice = U[0] << (uint32_t)(-dd);
+          } else {
+            const int64_t q = dd >> 5;
+            const uint32_t sh = (uint32_t)(dd & 31);
+            const uint32_t lo = q < P ? U[q] : 0u;
+            const uint32_t hi = q + 1 < P ? U[q + 1] : 0u;
+            slice = __funnelshift_r(lo, hi, sh);
+          }
+          sw += slice;
+          if (sS[c] && (bi >> 5) + P == w) sw -= (int64_t)1 << (bi & 31);
+        }
+      }
+      const uint32_t lo = (uint32_t)sw;
+      const int hi = (int)(sw >> 32);
+      // hi of word w-1
+      int hprev = __shfl_up_sync(0xffffffffu, hi, 1);
+      if (lane == 31) s_warp_hi[wid] = hi;
+      __syncthreads();
+      if (lane == 0) hprev = (wid == 0) ? s_hi_prev : s_warp_hi[wid - 1];
+      const int64_t z = (int64_t)lo + hprev;
+      const uint32_t y = (uint32_t)z;
+      const int g = (int)(z >> 32);
+      uint32_t f = active ? word_tf(y, g) : kTfIdentity;
+      // inclusive warp scan of transfer functions
+      uint32_t inc = f;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc = compose_tf(inc, u);
+      }
+      if (lane == 31) s_warp_tf[wid] = inc;
+      uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) exc = kTfIdentity;
+      __syncthreads();
+      // prefix of earlier warps
+      uint32_t wp = kTfIdentity;
+      for (int q = 0; q < wid; ++q) wp = compose_tf(s_warp_tf[q], wp);
+      const int cin_block = s_carry;
+      const int cin = apply_tf(compose_tf(exc, wp), cin_block);
+      if (active) {
+        const uint32_t F = y + (uint32_t)cin;
+        o[w] = F;
+        if (F != 0u) {
+          if ((int)w < first_nz) first_nz = (int)w;
+          if ((int)w > last_nz) last_nz = (int)w;
+        }
+        if (F != 0xffffffffu && (int)w > last_no) last_no = (int)w;
+        if (w == W - 1) s_top = F;
+      }
+      __syncthreads();
+      if (tid == bs - 1) {
+        uint32_t tot = kTfIdentity;
+        for (int q = 0; q < bs / 32; ++q) tot = compose_tf(s_warp_tf[q], tot);
+        s_carry = apply_tf(tot, cin_block);
+        s_hi_prev = hi;
+      }
+      __syncthreads();
+    }
+  }
+
+  atomicMin(&s_first_nz, first_nz);
+  atomicMax(&s_last_nz, last_nz);
+  atomicMax(&s_last_no, last_no);
+  __syncthreads();
+  const bool negative = W > 0 && (s_top >> 31);
+  int top;
+  if (negative) {
+    const int zf = s_first_nz;  // exists: a negative value is nonzero
+    for (int64_t w = zf + tid; w < W; w += bs) {
+      const uint32_t F = o[w];
+      o[w] = (w == zf) ? (0u - F) : ~F;
+    }
+    top = s_last_no > zf ? s_last_no : zf;
+  } else {
+    top = s_last_nz;
+  }
+  if (tid == 0) {
+    const int limbs = top >= 0 ? top / 2 + 1 : 0;
+    out_sizes[d.entry] = negative ? -limbs : limbs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt) {
+  cudaError_t e = cudaMemcpyToSymbol(c_primes, primes, sizeof(PrimeConst) * kMaxPrimes);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(c_crt, crt, sizeof(CrtConst));
+}
+
+static int ntt_threads(int lgN) {
+  const int half = 1 << (lgN - 1);
+  return half < 32 ? 32 : (half > 1024 ? 1024 : half);
+}
+
+cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
+                             int lgN, const uint64_t* limbs, uint32_t* res,
+                             const uint2* twf, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  const size_t smem = sizeof(uint32_t) << lgN;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 grid(count, P);
+  k_split_fwd<<<grid, ntt_threads(lgN), smem, st>>>(descs, idx, limbs, res, twf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count, int P,
+                           int lgN, uint32_t* res, const uint2* twi, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  const size_t smem = sizeof(uint32_t) << lgN;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 grid(count, P);
+  k_inv_ntt<<<grid, ntt_threads(lgN), smem, st>>>(descs, idx, res, twi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, int count,
+                            uint32_t* res, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  k_contract<<<count, kContractThreads, 0, st>>>(prods, items, res);
+  return cudaGetLastError();
+}
+
+int contract_block_freqs() { return kContractThreads; }
+int recompose_threads() { return kRecThreads; }
+
+template <int P>
+static cudaError_t launch_rec_t(const InvDesc* descs, const uint32_t* idx, int count,
+                                const uint32_t* res, uint32_t* out, int32_t* sizes,
+                                int words_per_thread, size_t smem, cudaStream_t st) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_crt_recompose<P>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_crt_recompose<P><<<count, kRecThreads, smem, st>>>(descs, idx, res, out, sizes,
+                                                       words_per_thread);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int count, int P,
+                                 const uint32_t* res, uint32_t* out, int32_t* sizes,
+                                 int words_per_thread, size_t smem, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  switch (P) {
+#define MPZMM_REC_CASE(PP) \
+  case PP:                 \
+    return launch_rec_t<PP>(descs, idx, count, res, out, sizes, words_per_thread, smem, st);
+    MPZMM_REC_CASE(2)
+    MPZMM_REC_CASE(3)
+    MPZMM_REC_CASE(4)
+    MPZMM_REC_CASE(5)
+    MPZMM_REC_CASE(6)
+    MPZMM_REC_CASE(7)
+    MPZMM_REC_CASE(8)
+    MPZMM_REC_CASE(9)
+    MPZMM_REC_CASE(10)
+    MPZMM_REC_CASE(11)
+    MPZMM_REC_CASE(12)
+    MPZMM_REC_CASE(13)
+    MPZMM_REC_CASE(14)
+    MPZMM_REC_CASE(15)
+    MPZMM_REC_CASE(16)
+#undef MPZMM_REC_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace mpzmm

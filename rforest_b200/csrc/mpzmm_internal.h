@@ -1,0 +1,91 @@
+// Internal types shared by the host engine and the sm_100a kernels.
+//
+// Residue arithmetic runs modulo word-size NTT primes p < 2^30 with
+// p = 1 (mod 2^20), so that 4p < 2^32 (lazy 32-bit Montgomery/Shoup
+// arithmetic) and p^2 < 2^60 (sixteen products accumulate exactly in 64 bits).
+// The reference's 62-bit primes (src/include/fft62.h:24-31) would force
+// multi-instruction 64-bit products on CUDA cores; the result is the same
+// exact integer either way.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace mpzmm {
+
+constexpr int kMaxPrimes = 16;      // primes available to a product
+constexpr int kPrimeLgRoot = 20;    // every prime is 1 mod 2^20
+constexpr int kMaxLgN = 15;         // largest transform handled in one CTA
+constexpr int kTwiddleLg = kMaxLgN; // twiddle tables cover N <= 2^kTwiddleLg
+constexpr int kMaxCoeffBits = 192;  // largest split coefficient (r)
+constexpr int kMaxCrtWords = kMaxPrimes + 1;  // 32-bit words of a CRT value
+
+// Per-prime constants, in __constant__ memory on the device.
+struct PrimeConst {
+  uint32_t p;        // the prime
+  uint32_t pinv;     // -p^{-1} mod 2^32 (Montgomery)
+  uint32_t r2;       // 2^64 mod p
+  uint32_t mu;       // floor(2^32 / p) (Barrett for 32-bit words)
+  uint32_t b32;      // 2^32 mod p
+  uint32_t b32q;     // Shoup companion of b32
+  uint32_t post;     // factor applied before CRT: 2^32 * N^{-1} is folded per
+  uint32_t pad;      //   launch, so this slot is unused on the device
+};
+
+// Garner constants for the first P primes: mixed-radix digits
+//   x = v0 + v1 p0 + v2 p0 p1 + ...
+// v_i = (x_i - (v0 + v1 p0 + ... )) * inv_i mod p_i with inv_i = (p0...p_{i-1})^{-1}.
+struct CrtConst {
+  uint32_t pmod[kMaxPrimes][kMaxPrimes];   // pmod[i][a] = p_a mod p_i  (a < i)
+  uint32_t pmodq[kMaxPrimes][kMaxPrimes];  // Shoup companions
+  uint32_t inv[kMaxPrimes];                // (p0...p_{i-1})^{-1} mod p_i
+  uint32_t invq[kMaxPrimes];
+  // M_P = p0...p_{P-1} and floor(M_P / 2) as little-endian 32-bit words
+  uint32_t M[kMaxPrimes + 1][kMaxCrtWords];
+  uint32_t Mhalf[kMaxPrimes + 1][kMaxCrtWords];
+  int Mwords[kMaxPrimes + 1];              // words of M_P
+};
+
+// One polynomial (one matrix entry) of the forward transform.
+struct FwdDesc {
+  uint64_t limb_off;   // first limb in the input limb buffer
+  uint64_t res_off;    // first residue word (prime 0); prime j at + j*N
+  int32_t size;        // signed limb count (GMP convention)
+  uint32_t r;          // coefficient width in bits
+  uint16_t lgN;
+  uint16_t P;
+  uint32_t ncoef;      // coefficients to split (<= N)
+};
+
+// One output polynomial of the inverse transform + CRT + recompose.
+struct InvDesc {
+  uint64_t res_off;
+  uint64_t out_word;   // first 32-bit output word
+  uint32_t out_words;  // output words (even: whole 64-bit limbs)
+  uint32_t r;
+  uint32_t ncoef;      // coefficients that can be nonzero
+  uint16_t lgN;
+  uint16_t P;
+  uint32_t entry;      // output entry index (for the size array)
+};
+
+// One product of the contraction (per frequency: C = A B mod p).
+struct ProdDesc {
+  uint64_t a_res;      // residue offset of A's poly 0 (row-major m x k)
+  uint64_t b_res;      // of B's poly 0 (k x n)
+  uint64_t c_res;      // of C's poly 0 (m x n)
+  uint16_t m, k, n;
+  uint16_t lgN;
+  uint16_t P;
+  uint16_t pad;
+};
+
+// Work item of the contraction: one product, one prime, one frequency block.
+struct ContractItem {
+  uint32_t prod;
+  uint16_t prime;
+  uint16_t pad;
+  uint32_t h0;         // first frequency of the block
+};
+
+}  // namespace mpzmm

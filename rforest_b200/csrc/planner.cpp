@@ -1,0 +1,238 @@
+// Prime tables, twiddle tables, Garner constants and parameter selection.
+//
+// The reference uses fixed 62-bit primes (src/include/fft62.h:24-31) and
+// picks (r, lgN) with a double-precision loop (src/lib/mpnfft.c:18-78).  Here
+// the primes are found at set-up (deterministic Miller-Rabin), and the
+// parameter choice is integer-only with an explicit exactness bound.
+#include "planner.h"
+
+#include <cstring>
+#include <mutex>
+
+namespace mpzmm {
+
+namespace {
+
+uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
+  uint64_t r = 1 % p;
+  a %= p;
+  while (e) {
+    if (e & 1) r = r * a % p;
+    a = a * a % p;
+    e >>= 1;
+  }
+  return r;
+}
+
+// Deterministic for n < 3,215,031,751 with bases 2, 3, 5, 7 (Pomerance,
+// Selfridge and Wagstaff); all candidates here are below 2^30.
+bool is_prime(uint32_t n) {
+  if (n < 2) return false;
+  for (uint32_t q : {2u, 3u, 5u, 7u, 11u, 13u}) {
+    if (n % q == 0) return n == q;
+  }
+  uint32_t d = n - 1;
+  int s = 0;
+  while ((d & 1) == 0) {
+    d >>= 1;
+    ++s;
+  }
+  for (uint64_t a : {2ull, 3ull, 5ull, 7ull}) {
+    uint64_t x = powmod(a, d, n);
+    if (x == 1 || x == n - 1) continue;
+    bool comp = true;
+    for (int i = 1; i < s; ++i) {
+      x = x * x % n;
+      if (x == n - 1) {
+        comp = false;
+        break;
+      }
+    }
+    if (comp) return false;
+  }
+  return true;
+}
+
+uint32_t primitive_root(uint32_t p) {
+  // factor p - 1
+  std::vector<uint32_t> f;
+  uint32_t m = p - 1;
+  for (uint32_t q = 2; q * q <= m; ++q) {
+    if (m % q == 0) {
+      f.push_back(q);
+      while (m % q == 0) m /= q;
+    }
+  }
+  if (m > 1) f.push_back(m);
+  for (uint32_t g = 2;; ++g) {
+    bool ok = true;
+    for (uint32_t q : f) {
+      if (powmod(g, (p - 1) / q, p) == 1) {
+        ok = false;
+        break;
+      }
+    }
+    if (ok) return g;
+  }
+}
+
+uint32_t shoup(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
+
+uint32_t brev(uint32_t x, int bits) {
+  uint32_t r = 0;
+  for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
+
+// little-endian 32-bit word vectors
+void mul_small(std::vector<uint32_t>& x, uint32_t v) {
+  uint64_t cy = 0;
+  for (auto& w : x) {
+    uint64_t t = (uint64_t)w * v + cy;
+    w = (uint32_t)t;
+    cy = t >> 32;
+  }
+  if (cy) x.push_back((uint32_t)cy);
+}
+
+Moduli* g_moduli = nullptr;
+std::once_flag g_once;
+
+void build(Moduli& M) {
+  int cnt = 0;
+  for (uint32_t c = (1u << (30 - kPrimeLgRoot)) - 1; c > 0 && cnt < kMaxPrimes; --c) {
+    uint32_t p = (c << kPrimeLgRoot) + 1;
+    if (p < (1u << 30) && is_prime(p)) M.p[cnt++] = p;
+  }
+  std::memset(M.pc, 0, sizeof(M.pc));
+  std::memset(&M.crt, 0, sizeof(M.crt));
+  const int TS = 1 << kTwiddleLg;
+  M.twf.assign((size_t)kMaxPrimes * TS, make_uint2(0, 0));
+  M.twi.assign((size_t)kMaxPrimes * TS, make_uint2(0, 0));
+  for (int j = 0; j < kMaxPrimes; ++j) {
+    const uint32_t p = M.p[j];
+    PrimeConst& pc = M.pc[j];
+    pc.p = p;
+    uint32_t inv = p;  // Newton iteration for p^{-1} mod 2^32 (p odd)
+    for (int i = 0; i < 5; ++i) inv *= 2 - p * inv;
+    pc.pinv = (uint32_t)(0u - inv);
+    pc.r2 = (uint32_t)(((unsigned __int128)1 << 64) % p);
+    pc.mu = (uint32_t)((((uint64_t)1) << 32) / p);
+    pc.b32 = (uint32_t)((((uint64_t)1) << 32) % p);
+    pc.b32q = shoup(pc.b32, p);
+    const uint32_t g = primitive_root(p);
+    const uint64_t wmax = powmod(g, (p - 1) >> kTwiddleLg, p);  // order 2^kTwiddleLg
+    for (int lgm = 0; lgm < kTwiddleLg; ++lgm) {
+      const uint32_t m = 1u << lgm;
+      // w_{2m} = wmax^(TS / (2m))
+      const uint64_t w2m = powmod(wmax, (uint64_t)TS >> (lgm + 1), p);
+      const uint64_t w2mi = powmod(w2m, p - 2, p);
+      for (uint32_t i = 0; i < m; ++i) {
+        const uint32_t e = brev(i, lgm);
+        const uint32_t w = (uint32_t)powmod(w2m, e, p);
+        const uint32_t wi = (uint32_t)powmod(w2mi, e, p);
+        M.twf[(size_t)j * TS + m + i] = make_uint2(w, shoup(w, p));
+        M.twi[(size_t)j * TS + m + i] = make_uint2(wi, shoup(wi, p));
+      }
+    }
+  }
+  // Garner constants
+  for (int i = 1; i < kMaxPrimes; ++i) {
+    const uint32_t p = M.p[i];
+    uint64_t prod = 1;
+    for (int a = 0; a < i; ++a) {
+      const uint32_t pm = M.p[a] % p;
+      M.crt.pmod[i][a] = pm;
+      M.crt.pmodq[i][a] = shoup(pm, p);
+      prod = prod * pm % p;
+    }
+    const uint32_t iv = (uint32_t)powmod(prod, p - 2, p);
+    M.crt.inv[i] = iv;
+    M.crt.invq[i] = shoup(iv, p);
+  }
+  std::vector<uint32_t> acc{1};
+  for (int P = 1; P <= kMaxPrimes; ++P) {
+    mul_small(acc, M.p[P - 1]);
+    int words = (int)acc.size();
+    M.crt.Mwords[P] = words;
+    for (int q = 0; q < words && q < kMaxCrtWords; ++q) M.crt.M[P][q] = acc[q];
+    for (int q = 0; q < words && q < kMaxCrtWords; ++q) {
+      uint32_t hi = (q + 1 < words) ? acc[q + 1] : 0u;
+      M.crt.Mhalf[P][q] = (acc[q] >> 1) | (hi << 31);
+    }
+    int top = 31;
+    while (!((acc.back() >> top) & 1u)) --top;
+    M.mbits[P] = 32 * (words - 1) + top;  // floor(log2 M)
+  }
+  M.mbits[0] = 0;
+}
+
+}  // namespace
+
+const Moduli& moduli() {
+  std::call_once(g_once, [] {
+    g_moduli = new Moduli;
+    build(*g_moduli);
+  });
+  return *g_moduli;
+}
+
+int ceil_log2(uint64_t x) {
+  int b = 0;
+  while (((uint64_t)1 << b) < x) ++b;
+  return b;
+}
+
+int64_t output_limbs(int k, int64_t a_bits, int64_t b_bits) {
+  if (k <= 0 || a_bits <= 0 || b_bits <= 0) return 1;
+  return (a_bits + b_bits + ceil_log2((uint64_t)k) + 1 + 63) / 64;
+}
+
+bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* out) {
+  *out = Params();
+  if (a_bits <= 0 || b_bits <= 0 || k <= 0 || m <= 0 || n <= 0) {
+    out->out_limbs = 1;
+    return true;  // identically zero product: P = 0
+  }
+  const Moduli& M = moduli();
+  const int clk = ceil_log2((uint64_t)k);
+  const int64_t nfwd = (int64_t)m * k + (int64_t)k * n;
+  const int64_t ninv = (int64_t)m * n;
+  int64_t best = -1;
+  for (int P = 2; P <= kMaxPrimes; ++P) {
+    const int budget = M.mbits[P] - 1 - clk;  // 2r + ceil(log2 minlen) <= budget
+    if (budget < 3) continue;
+    int r = budget / 2;
+    if (r > kMaxCoeffBits) r = kMaxCoeffBits;
+    int64_t lenA = 0, lenB = 0;
+    for (; r >= 1; --r) {
+      lenA = (a_bits + r - 1) / r;
+      lenB = (b_bits + r - 1) / r;
+      const int64_t mn = lenA < lenB ? lenA : lenB;
+      if (2 * r + ceil_log2((uint64_t)mn) <= budget) break;
+    }
+    if (r < 1) continue;
+    const int64_t len = lenA + lenB - 1;
+    int lgN = ceil_log2((uint64_t)len);
+    if (lgN < 2) lgN = 2;
+    if (lgN > kMaxLgN) continue;
+    // per (prime, frequency) work: transforms, contraction, CRT/recompose
+    const int64_t Nn = (int64_t)1 << lgN;
+    const int64_t cost = P * Nn *
+                         ((nfwd + ninv) * (5 * lgN + 12) + 2 * (int64_t)m * n * k +
+                          ninv * (3 * P + 10));
+    if (best < 0 || cost < best) {
+      best = cost;
+      out->P = P;
+      out->r = r;
+      out->lgN = lgN;
+      out->lenA = lenA;
+      out->lenB = lenB;
+    }
+  }
+  if (best < 0) return false;
+  out->out_limbs = output_limbs(k, a_bits, b_bits);
+  return true;
+}
+
+}  // namespace mpzmm
