@@ -20,16 +20,27 @@ class MpzStruct(C.Structure):
                 ("_mp_d", C.POINTER(C.c_uint64))]
 
 
-def gmp():
+class _Gmp:
+    """The four GMP routines used here, looked up by their exported names
+    (attribute access would be name-mangled inside classes)."""
+
+    def __init__(self):
+        g = C.CDLL("libgmp.so.10")
+        self.init = getattr(g, "__gmpz_init")
+        self.init.argtypes = [C.c_void_p]
+        self.clear = getattr(g, "__gmpz_clear")
+        self.clear.argtypes = [C.c_void_p]
+        self.limbs_write = getattr(g, "__gmpz_limbs_write")
+        self.limbs_write.argtypes = [C.c_void_p, C.c_long]
+        self.limbs_write.restype = C.POINTER(C.c_uint64)
+        self.limbs_finish = getattr(g, "__gmpz_limbs_finish")
+        self.limbs_finish.argtypes = [C.c_void_p, C.c_long]
+
+
+def gmp() -> _Gmp:
     global _gmp
     if _gmp is None:
-        g = C.CDLL("libgmp.so.10")
-        g.__gmpz_init.argtypes = [C.c_void_p]
-        g.__gmpz_clear.argtypes = [C.c_void_p]
-        g.__gmpz_limbs_write.argtypes = [C.c_void_p, C.c_long]
-        g.__gmpz_limbs_write.restype = C.POINTER(C.c_uint64)
-        g.__gmpz_limbs_finish.argtypes = [C.c_void_p, C.c_long]
-        _gmp = g
+        _gmp = _Gmp()
     return _gmp
 
 
@@ -42,7 +53,7 @@ class MpzArray:
         self.arr = (MpzStruct * self.n)()
         g = gmp()
         for i in range(self.n):
-            g.__gmpz_init(C.byref(self.arr[i]))
+            g.init(C.byref(self.arr[i]))
         for i, v in enumerate(vals):
             self.set(i, v)
 
@@ -51,11 +62,11 @@ class MpzArray:
         nl = (mag.bit_length() + 63) // 64
         g = gmp()
         if nl == 0:
-            g.__gmpz_limbs_finish(C.byref(self.arr[i]), 0)
+            g.limbs_finish(C.byref(self.arr[i]), 0)
             return
-        d = g.__gmpz_limbs_write(C.byref(self.arr[i]), nl)
+        d = g.limbs_write(C.byref(self.arr[i]), nl)
         C.memmove(d, mag.to_bytes(8 * nl, "little"), 8 * nl)
-        g.__gmpz_limbs_finish(C.byref(self.arr[i]), -nl if v < 0 else nl)
+        g.limbs_finish(C.byref(self.arr[i]), -nl if v < 0 else nl)
 
     def get(self, i: int) -> int:
         z = self.arr[i]
@@ -75,7 +86,7 @@ class MpzArray:
         if self.arr is not None:
             g = gmp()
             for i in range(self.n):
-                g.__gmpz_clear(C.byref(self.arr[i]))
+                g.clear(C.byref(self.arr[i]))
             self.arr = None
 
     def __del__(self):

@@ -97,3 +97,12 @@ def test_compute_without_device_fails_loudly(product_lib):
     with pytest.raises(_lib.MpzmmError) as e:
         api.matmul(1, 2, 1, A, B)
     assert e.value.status == _lib.MPZMM_ERR_CUDA
+
+
+def test_mpz_array_roundtrip():
+    """mpz_t arrays built through the GMP runtime keep their values."""
+    from rforest_b200 import gmp
+    vals = [0, 1, -1, (1 << 64) - 1, -(1 << 200) + 3, 1 << 4096]
+    a = gmp.MpzArray(vals)
+    assert a.to_ints() == vals
+    a.close()
