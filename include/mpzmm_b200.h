@@ -169,6 +169,33 @@ MPZMM_API int mpzmm_plan_stage_times(mpzmm_plan *plan, float *ms4, int64_t *laun
 MPZMM_API int mpzmm_plan_info(const mpzmm_plan *plan, int64_t *launches_per_execute,
                     int64_t *device_bytes, int index, int *P, int *r, int *lgN);
 
+/* Exact C = A * B without allocating anything: no counterpart in the
+   reference.  For callers that cannot allocate device memory -- a process
+   whose GPU memory is all owned by a host framework's pool, where a raw
+   cudaMalloc fails or escapes the pool's accounting, or a latency-sensitive
+   path that cannot pay for cudaMalloc/cudaFree, which may synchronise the
+   whole device.  The caller passes device buffers: d_a_limbs / d_b_limbs
+   hold the operands' limbs (entry offsets and signed sizes in the HOST
+   arrays a_offs/a_sizes, b_offs/b_sizes); results go to d_c_limbs at the
+   HOST offsets c_offs with HOST capacities c_caps, and their signed sizes to
+   the DEVICE array d_c_sizes.  Every capacity must be at least
+   mpzmm_output_limbs(k, 64 * max |a_sizes|, 64 * max |b_sizes|).
+   Scratch is a fixed 16 MiB static device array inside the library (plus
+   8 MiB of static transform tables), held on every GPU that loads the
+   library until exit; products needing more scratch, or a transform longer
+   than 2^15 points, are rejected with MPZMM_ERR_TOO_LARGE.  The first call
+   on a device sets up that device's tables (make it before any stream
+   capture).  All calls share the one scratch array and leave their data in
+   it: calls whose GPU work overlaps race, so serialise them.  Asynchronous
+   on `stream` (NULL: the legacy default stream). */
+MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
+                                   const uint64_t *d_a_limbs, const int64_t *a_offs,
+                                   const int32_t *a_sizes,
+                                   const uint64_t *d_b_limbs, const int64_t *b_offs,
+                                   const int32_t *b_sizes,
+                                   uint64_t *d_c_limbs, const int64_t *c_offs,
+                                   const int64_t *c_caps, int32_t *d_c_sizes, void *stream);
+
 /* Parameters (prime count P, coefficient bits r, transform length 2^lgN)
    that the planner picks for a product with k terms whose A and B entries
    have at most a_bits and b_bits bits.  Host-only; no device needed. */

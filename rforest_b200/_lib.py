@@ -81,6 +81,8 @@ def lib():
         "mpzmm_plan_stage_times": (C.c_int, [vp, C.POINTER(C.c_float), i64p, i64p]),
         "mpzmm_plan_info": (C.c_int, [vp, i64p, i64p, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "mpzmm_matmul_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, i64p, i32p, vp, i64p,
+                                           i32p, vp, i64p, i64p, vp, vp]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }
