@@ -287,7 +287,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     pd.n = (uint16_t)n;
     pd.lgN = (uint16_t)lgN;
     pd.P = (uint16_t)P;
-    pd.pad = 0;
+    pd.pad = (uint16_t)((m >= 3 ? 2 : 0) + (n >= 3 ? 1 : 0));  // contraction tile
     pd.a_res = n_res_;
     n_res_ += (uint64_t)m * k * poly;
     pd.b_res = n_res_;
@@ -309,9 +309,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
         fd.P = (uint16_t)P;
         uint64_t nc = ((uint64_t)nl * 64 + r - 1) / r;
         fd.ncoef = (uint32_t)(nc < N ? nc : N);
-        auto& g = fwdg[{lgN, P}];
+        auto& g = fwdg[{lgN, P * 16 + (r + 29) / 30}];
         g.P = P;
         g.lgN = lgN;
+        if (r > g.max_r) g.max_r = r;
         g.idx.push_back((uint32_t)fwd_.size());
         fwd_.push_back(fd);
       }
@@ -466,7 +467,7 @@ int Plan::execute(cudaStream_t st) {
   }
   for (const Group& g : fwd_groups_)
     CU(launch_split_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN,
-                        ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
+                        ws_->d_limbs, ws_->d_res, ctx.d_twf, st, g.max_r),
        "split+forward NTT launch");
   if (timing_) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
   if (!items_.empty())

@@ -122,6 +122,7 @@ class Plan {
  private:
   struct Group {
     int P = 0, lgN = 0;
+    int max_r = 0;         // widest coefficient of the group (split kernels)
     uint32_t idx_off = 0;  // into the device index array
     std::vector<uint32_t> idx;
     int words_per_thread = 1;

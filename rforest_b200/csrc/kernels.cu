@@ -22,6 +22,7 @@
 #include "kernels.h"
 #include "modarith.cuh"
 #include "mpzmm_internal.h"
+#include "ntt_fast.cuh"
 
 namespace mpzmm {
 
@@ -154,23 +155,21 @@ __global__ void k_inv_ntt(const InvDesc* __restrict__ descs,
 
 // ---------------------------------------------------------------------------
 // Contraction on CUDA cores.  One thread per frequency h; it walks the m x n
-// outputs in strips of 4 columns.  Products of residues < p < 2^30 are < 2^60,
-// so sixteen of them accumulate exactly in 64 bits before a Montgomery fold
-// (the reference reduces every 16 terms for the same reason with 128-bit
+// outputs in register tiles of TI x TJ (2 or 4 each, chosen per product and
+// stored in ProdDesc::pad), loading TI + TJ residues per TI * TJ products.
+// Edge tiles clamp their row/column to the last one (in-bounds duplicate
+// work, results discarded).  Products of residues < p < 2^30 are < 2^60, so
+// sixteen of them accumulate exactly in 64 bits before a Montgomery fold (the
+// reference reduces every 16 terms for the same reason with 128-bit
 // accumulators, src/lib/mpnfft.c:621-627).  Outputs carry a factor 2^-32
 // that the CRT stage removes.
 // ---------------------------------------------------------------------------
 constexpr int kContractThreads = 128;
 
-__global__ void __launch_bounds__(kContractThreads)
-k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
-           uint32_t* __restrict__ res) {
-  const ContractItem it = items[blockIdx.x];
-  const ProdDesc d = prods[it.prod];
+template <int TI, int TJ>
+__device__ __forceinline__ void contract_tiles(const ProdDesc& d, int j, uint32_t h,
+                                               uint32_t* __restrict__ res) {
   const int N = 1 << d.lgN;
-  const uint32_t h = it.h0 + threadIdx.x;
-  if (h >= (uint32_t)N) return;
-  const int j = it.prime;
   const uint32_t p = c_primes[j].p;
   const uint32_t pinv = c_primes[j].pinv;
   const uint32_t mu = c_primes[j].mu;
@@ -180,41 +179,76 @@ k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ 
   const uint32_t* __restrict__ B = res + d.b_res + base;
   uint32_t* C = res + d.c_res + base;
   const int m = d.m, k = d.k, n = d.n;
-  for (int i = 0; i < m; ++i) {
-    const uint32_t* Arow = A + (uint64_t)(i * k) * stride;
-    for (int l0 = 0; l0 < n; l0 += 4) {
-      const int nc = (n - l0) < 4 ? (n - l0) : 4;
-      uint64_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
-      uint32_t s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-      int cnt = 0;
-      for (int kk = 0; kk < k; ++kk) {
-        const uint32_t a = __ldg(Arow + (uint64_t)kk * stride);
-        const uint32_t* Bk = B + (uint64_t)(kk * n + l0) * stride;
-        acc0 += (uint64_t)a * __ldg(Bk);
-        if (nc > 1) acc1 += (uint64_t)a * __ldg(Bk + stride);
-        if (nc > 2) acc2 += (uint64_t)a * __ldg(Bk + 2 * stride);
-        if (nc > 3) acc3 += (uint64_t)a * __ldg(Bk + 3 * stride);
-        if (++cnt == 16) {
-          s0 = add_mod(s0, redc64(acc0, p, pinv, mu), p);
-          s1 = add_mod(s1, redc64(acc1, p, pinv, mu), p);
-          s2 = add_mod(s2, redc64(acc2, p, pinv, mu), p);
-          s3 = add_mod(s3, redc64(acc3, p, pinv, mu), p);
-          acc0 = acc1 = acc2 = acc3 = 0;
-          cnt = 0;
+  const uint64_t bstep = (uint64_t)n * stride;
+  for (int i0 = 0; i0 < m; i0 += TI) {
+    for (int l0 = 0; l0 < n; l0 += TJ) {
+      const uint32_t* Ap[TI];
+      const uint32_t* Bp[TJ];
+#pragma unroll
+      for (int x = 0; x < TI; ++x) {
+        const int ii = (i0 + x) < m ? (i0 + x) : (m - 1);
+        Ap[x] = A + (uint64_t)ii * k * stride;
+      }
+#pragma unroll
+      for (int y = 0; y < TJ; ++y) {
+        const int ll = (l0 + y) < n ? (l0 + y) : (n - 1);
+        Bp[y] = B + (uint64_t)ll * stride;
+      }
+      uint32_t sum[TI][TJ];
+#pragma unroll
+      for (int x = 0; x < TI; ++x)
+#pragma unroll
+        for (int y = 0; y < TJ; ++y) sum[x][y] = 0;
+      for (int k0 = 0; k0 < k; k0 += 16) {
+        const int k1 = (k0 + 16) < k ? (k0 + 16) : k;
+        uint64_t acc[TI][TJ];
+#pragma unroll
+        for (int x = 0; x < TI; ++x)
+#pragma unroll
+          for (int y = 0; y < TJ; ++y) acc[x][y] = 0;
+        for (int q = k0; q < k1; ++q) {
+          uint32_t av[TI], bv[TJ];
+#pragma unroll
+          for (int x = 0; x < TI; ++x) av[x] = __ldg(Ap[x] + (uint64_t)q * stride);
+#pragma unroll
+          for (int y = 0; y < TJ; ++y) bv[y] = __ldg(Bp[y] + (uint64_t)q * bstep);
+#pragma unroll
+          for (int x = 0; x < TI; ++x)
+#pragma unroll
+            for (int y = 0; y < TJ; ++y) acc[x][y] += (uint64_t)av[x] * bv[y];
+        }
+#pragma unroll
+        for (int x = 0; x < TI; ++x)
+#pragma unroll
+          for (int y = 0; y < TJ; ++y)
+            sum[x][y] = add_mod(sum[x][y], redc64(acc[x][y], p, pinv, mu), p);
+      }
+#pragma unroll
+      for (int x = 0; x < TI; ++x) {
+        if (i0 + x >= m) continue;
+#pragma unroll
+        for (int y = 0; y < TJ; ++y) {
+          if (l0 + y >= n) continue;
+          C[((uint64_t)(i0 + x) * n + (l0 + y)) * stride] = sum[x][y];
         }
       }
-      if (cnt) {
-        s0 = add_mod(s0, redc64(acc0, p, pinv, mu), p);
-        s1 = add_mod(s1, redc64(acc1, p, pinv, mu), p);
-        s2 = add_mod(s2, redc64(acc2, p, pinv, mu), p);
-        s3 = add_mod(s3, redc64(acc3, p, pinv, mu), p);
-      }
-      uint32_t* Cr = C + (uint64_t)(i * n + l0) * stride;
-      Cr[0] = s0;
-      if (nc > 1) Cr[stride] = s1;
-      if (nc > 2) Cr[2 * stride] = s2;
-      if (nc > 3) Cr[3 * stride] = s3;
     }
+  }
+}
+
+__global__ void __launch_bounds__(kContractThreads)
+k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
+           uint32_t* __restrict__ res) {
+  const ContractItem it = items[blockIdx.x];
+  const ProdDesc d = prods[it.prod];
+  const int N = 1 << d.lgN;
+  const uint32_t h = it.h0 + threadIdx.x;
+  if (h >= (uint32_t)N) return;
+  switch (d.pad) {  // tile shape, uniform over the CTA
+    case 3: contract_tiles<4, 4>(d, it.prime, h, res); break;
+    case 2: contract_tiles<4, 2>(d, it.prime, h, res); break;
+    case 1: contract_tiles<2, 4>(d, it.prime, h, res); break;
+    default: contract_tiles<2, 2>(d, it.prime, h, res); break;
   }
 }
 
@@ -482,6 +516,160 @@ k_crt_recompose(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Split + forward NTT, register-blocked (lgN >= 3).
+//
+// 256 threads per CTA.  Small transforms (N <= 2048) are packed several per
+// CTA: a team of N/8 threads owns one entry and each thread the 8 points
+// x = q N/8 + t of the first pass, whose 30-bit coefficient digits it
+// extracts once and keeps in registers for all P primes.  A residue is
+//     c mod p = REDC( sum_q d_q * (2^(30 q + 32) mod p) )
+// (D products of 30-bit by 30-bit numbers, exact in 64 bits for D <= 8), so
+// each prime costs D wide multiply-adds and one Montgomery reduction instead
+// of a Horner chain.  Larger transforms take a whole CTA and re-extract
+// digits per prime.  Then passes of 3 stages in registers (ntt_fast.cuh).
+// ---------------------------------------------------------------------------
+constexpr int kFwdThreads = 256;
+
+template <int D>
+__device__ __forceinline__ void coeff_digits(const uint32_t* __restrict__ w32, uint64_t nw,
+                                             uint64_t bit0, uint32_t r, bool live,
+                                             uint32_t (&dg)[D]) {
+#pragma unroll
+  for (int q = 0; q < D; ++q) {
+    const uint64_t b = bit0 + 30u * q;
+    const uint64_t wi = b >> 5;
+    const uint32_t sh = (uint32_t)(b & 31);
+    const uint32_t lo = (live && wi < nw) ? __ldg(w32 + wi) : 0u;
+    const uint32_t hi = (live && wi + 1 < nw) ? __ldg(w32 + wi + 1) : 0u;
+    uint32_t v = __funnelshift_r(lo, hi, sh) & 0x3fffffffu;
+    const int rem = (int)r - 30 * q;  // bits of the coefficient left for this digit
+    if (rem < 30) v = rem <= 0 ? 0u : (v & ((1u << rem) - 1u));
+    dg[q] = v;
+  }
+}
+
+template <int D>
+__device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int j, bool neg) {
+  const uint32_t p = c_primes[j].p;
+  uint64_t S = 0;
+#pragma unroll
+  for (int q = 0; q < D; ++q) S += (uint64_t)dg[q] * c_primes[j].dig[q];
+  const uint32_t v = redc64(S, p, c_primes[j].pinv, c_primes[j].mu);
+  return (neg && v) ? p - v : v;
+}
+
+template <int D, bool TEAM>
+__global__ void __launch_bounds__(kFwdThreads)
+k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
+       int lgN, int P, const uint64_t* __restrict__ limbs, uint32_t* __restrict__ res,
+       const uint2* __restrict__ twf) {
+  extern __shared__ uint32_t sm[];
+  const int N = 1 << lgN;
+  const int TS = TEAM ? (N >> 3) : kFwdThreads;  // threads per entry
+  const int team = TEAM ? (int)threadIdx.x / TS : 0;
+  const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
+  const int G = TEAM ? kFwdThreads / TS : 1;
+  const int slot = blockIdx.x * G + team;
+  const bool valid = slot < count;
+  uint32_t* s = sm + team * (N + (N >> 5));
+  FwdDesc d;
+  d.limb_off = 0;
+  d.res_off = 0;
+  d.size = 0;
+  d.r = 1;
+  d.ncoef = 0;
+  if (valid) d = descs[idx[slot]];
+  const uint64_t nw = 2ull * (uint64_t)(d.size < 0 ? -d.size : d.size);
+  const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
+  const bool neg = d.size < 0;
+  const int ng0 = N >> 3;  // groups (and the point stride) of the first pass
+
+  uint32_t dg[8][D];
+  if (TEAM) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int x = q * ng0 + tt;
+      coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
+    }
+  }
+  for (int j = 0; j < P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = twf + (size_t)j * kTwStride;
+    for (int g = tt; g < ng0; g += TS) {
+      uint32_t a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int x = q * ng0 + g;
+        if (!TEAM)
+          coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
+        a[q] = digits_residue<D>(dg[q], j, neg);
+      }
+      fwd_group<3>(a, 0, 0, tw, p);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s[smi(q * ng0 + g)] = a[q];
+    }
+    __syncthreads();
+    for (int s0 = 3; s0 < lgN; s0 += 3) {
+      const int Lp = (lgN - s0) < 3 ? (lgN - s0) : 3;
+      smem_pass<3, true>(s, lgN, s0, Lp, tt, TS, tw, p);
+      __syncthreads();
+    }
+    if (valid) {
+      uint32_t* out = res + d.res_off + (uint64_t)j * (uint64_t)N;
+      const uint32_t p2 = 2 * p;
+      for (int x = tt; x < N; x += TS) {
+        uint32_t v = reduce_2p(s[smi(x)], p2);
+        out[x] = v >= p ? v - p : v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
+template <bool TEAM>
+__global__ void __launch_bounds__(kFwdThreads)
+k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count, int lgN,
+       int P, uint32_t* __restrict__ res, const uint2* __restrict__ twi) {
+  extern __shared__ uint32_t sm[];
+  const int N = 1 << lgN;
+  const int TS = TEAM ? (N >> 3) : kFwdThreads;
+  const int team = TEAM ? (int)threadIdx.x / TS : 0;
+  const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
+  const int G = TEAM ? kFwdThreads / TS : 1;
+  const int slot = blockIdx.x * G + team;
+  const bool valid = slot < count;
+  uint32_t* s = sm + team * (N + (N >> 5));
+  const uint64_t off = valid ? descs[idx[slot]].res_off : 0;
+  const int last_s0 = ((lgN - 1) / 3) * 3;  // start of the last forward pass
+  for (int j = 0; j < P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = twi + (size_t)j * kTwStride;
+    uint32_t* io = res + off + (uint64_t)j * (uint64_t)N;
+    for (int x = tt; x < N; x += TS) s[smi(x)] = valid ? io[x] : 0u;
+    __syncthreads();
+    for (int s0 = last_s0; s0 >= 3; s0 -= 3) {
+      const int Lp = (lgN - s0) < 3 ? (lgN - s0) : 3;
+      smem_pass<3, false>(s, lgN, s0, Lp, tt, TS, tw, p);
+      __syncthreads();
+    }
+    // first forward pass (stages 0..2) inverted, straight to global memory
+    for (int g = tt; g < (N >> 3); g += TS) {
+      uint32_t a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = s[smi(q * (N >> 3) + g)];
+      inv_group<3>(a, 0, 0, tw, p);
+      if (valid) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) io[q * (N >> 3) + g] = a[q];  // in [0, 2p)
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -496,10 +684,49 @@ static int ntt_threads(int lgN) {
   return half < 32 ? 32 : (half > 1024 ? 1024 : half);
 }
 
+template <int D>
+static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx, int count, int P,
+                                 int lgN, const uint64_t* limbs, uint32_t* res, const uint2* twf,
+                                 cudaStream_t st) {
+  const int N = 1 << lgN;
+  const bool team = (N >> 3) <= kFwdThreads;
+  const int G = team ? kFwdThreads / (N >> 3) : 1;
+  const size_t smem = sizeof(uint32_t) * (size_t)G * (N + (N >> 5));
+  const int grid = (count + G - 1) / G;
+  if (team) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k_fwd2<D, true><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, limbs, res, twf);
+  } else {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k_fwd2<D, false><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, limbs, res, twf);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
                              int lgN, const uint64_t* limbs, uint32_t* res,
-                             const uint2* twf, cudaStream_t st) {
+                             const uint2* twf, cudaStream_t st, int max_r) {
   if (count == 0) return cudaSuccess;
+  if (lgN >= 3 && max_r >= 1 && max_r <= 7 * 30) {
+    switch ((max_r + 29) / 30) {
+      case 1: return launch_fwd2_d<1>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 2: return launch_fwd2_d<2>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 3: return launch_fwd2_d<3>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 4: return launch_fwd2_d<4>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 5: return launch_fwd2_d<5>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 6: return launch_fwd2_d<6>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      case 7: return launch_fwd2_d<7>(descs, idx, count, P, lgN, limbs, res, twf, st);
+      default: break;
+    }
+  }
   const size_t smem = sizeof(uint32_t) << lgN;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -514,6 +741,29 @@ cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int coun
 cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count, int P,
                            int lgN, uint32_t* res, const uint2* twi, cudaStream_t st) {
   if (count == 0) return cudaSuccess;
+  if (lgN >= 3) {
+    const int N = 1 << lgN;
+    const bool team = (N >> 3) <= kFwdThreads;
+    const int G = team ? kFwdThreads / (N >> 3) : 1;
+    const size_t smem = sizeof(uint32_t) * (size_t)G * (N + (N >> 5));
+    const int grid = (count + G - 1) / G;
+    if (team) {
+      if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(
+            k_inv2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+      }
+      k_inv2<true><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, res, twi);
+    } else {
+      if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(
+            k_inv2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+      }
+      k_inv2<false><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, res, twi);
+    }
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(uint32_t) << lgN;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,

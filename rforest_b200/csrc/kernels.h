@@ -11,9 +11,10 @@ cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt);
 
 // Split + forward NTT for `count` entries (descriptor indices idx[0..count)),
 // all with transform length 2^lgN and P primes.
+// max_r: the widest coefficient (bits) among the launch's entries.
 cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
                              int lgN, const uint64_t* limbs, uint32_t* res,
-                             const uint2* twf, cudaStream_t st);
+                             const uint2* twf, cudaStream_t st, int max_r);
 
 // Inverse NTT, in place, for `count` output entries of length 2^lgN.
 cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count, int P,

@@ -28,8 +28,10 @@ struct PrimeConst {
   uint32_t mu;       // floor(2^32 / p) (Barrett for 32-bit words)
   uint32_t b32;      // 2^32 mod p
   uint32_t b32q;     // Shoup companion of b32
-  uint32_t post;     // factor applied before CRT: 2^32 * N^{-1} is folded per
-  uint32_t pad;      //   launch, so this slot is unused on the device
+  uint32_t post;     // unused (the CRT scale 2^32 N^{-1} depends on N)
+  uint32_t pad;
+  uint32_t dig[8];   // 2^(30 q + 32) mod p: weights of the 30-bit digits of a
+                     // coefficient, with the Montgomery factor folded in
 };
 
 // Garner constants for the first P primes: mixed-radix digits
@@ -77,7 +79,7 @@ struct ProdDesc {
   uint16_t m, k, n;
   uint16_t lgN;
   uint16_t P;
-  uint16_t pad;
+  uint16_t pad;        // contraction register tile: bit 1 -> 4 rows, bit 0 -> 4 cols
 };
 
 // Work item of the contraction: one product, one prime, one frequency block.

@@ -171,7 +171,7 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   pd->n = (uint16_t)n;
   pd->lgN = (uint16_t)lgN;
   pd->P = (uint16_t)P;
-  pd->pad = 0;
+  pd->pad = (uint16_t)((m >= 3 ? 2 : 0) + (n >= 3 ? 1 : 0));  // contraction tile
   pd->a_res = 0;
   pd->b_res = (uint64_t)na * poly;
   pd->c_res = (uint64_t)(na + nb) * poly;
@@ -237,9 +237,9 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
       break;
     }
   }
-  if ((e = launch_split_fwd(dfwd, didx, (int)na, P, lgN, d_a_limbs, dres, ds->twf, s)) !=
+  if ((e = launch_split_fwd(dfwd, didx, (int)na, P, lgN, d_a_limbs, dres, ds->twf, s, r)) !=
           cudaSuccess ||
-      (e = launch_split_fwd(dfwd, didx + na, (int)nb, P, lgN, d_b_limbs, dres, ds->twf, s)) !=
+      (e = launch_split_fwd(dfwd, didx + na, (int)nb, P, lgN, d_b_limbs, dres, ds->twf, s, r)) !=
           cudaSuccess ||
       (e = launch_contract(dpd, ditems, (int)nitems, dres, s)) != cudaSuccess ||
       (e = launch_inv_ntt(dinv, didx + na + nb, (int)nc, P, lgN, dres, ds->twi, s)) !=
