@@ -359,22 +359,9 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   // launch groups and the shared index array
   for (auto& kv : fwdg) fwd_groups_.push_back(std::move(kv.second));
   for (auto& kv : invg) inv_groups_.push_back(std::move(kv.second));
-  const int rt = recompose_threads();
   for (auto& kv : recg) {
     Group g = std::move(kv.second);
-    const int64_t rmin = rec_min_r[g.P];
-    g.words_per_thread = 1;
-    for (int S : {8, 4, 2, 1}) {
-      const int64_t TW = (int64_t)rt * S;
-      const int64_t cmax = (32 * TW + 32 * g.P) / rmin + 3;
-      const int64_t bytes = cmax * (4 * g.P + 1);
-      if (bytes <= 96 * 1024 || S == 1) {
-        g.words_per_thread = S;
-        g.smem = (size_t)((bytes + 15) & ~15LL);
-        break;
-      }
-    }
-    if (g.smem > 200 * 1024) return set_error(kErrTooLarge, "coefficient width too small");
+    g.max_r = (int)rec_min_r[g.P];  // narrowest r: sizes the CRT kernel's scratch
     rec_groups_.push_back(std::move(g));
   }
   for (auto* gs : {&fwd_groups_, &inv_groups_, &rec_groups_})
@@ -480,7 +467,7 @@ int Plan::execute(cudaStream_t st) {
   if (timing_) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
   for (const Group& g : rec_groups_)
     CU(launch_crt_recompose(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, ws_->d_res,
-                            ws_->d_out, ws_->d_sizes, g.words_per_thread, g.smem, st),
+                            ws_->d_out, ws_->d_sizes, g.max_r, st),
        "CRT+recompose launch");
   if (timing_) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
   return kOk;

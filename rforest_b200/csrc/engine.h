@@ -122,11 +122,9 @@ class Plan {
  private:
   struct Group {
     int P = 0, lgN = 0;
-    int max_r = 0;         // widest coefficient of the group (split kernels)
+    int max_r = 0;         // split: widest coefficient; CRT: narrowest coefficient
     uint32_t idx_off = 0;  // into the device index array
     std::vector<uint32_t> idx;
-    int words_per_thread = 1;
-    size_t smem = 0;
   };
 
   std::vector<ProductSpec> prods_;

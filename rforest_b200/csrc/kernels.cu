@@ -268,7 +268,6 @@ k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ 
 // of the reference's serial borrow chain (src/lib/recompose.c:43-87) and of
 // its chunk fix-up (src/lib/crt_recompose.c:101-153).
 // ---------------------------------------------------------------------------
-constexpr int kRecThreads = 256;
 
 __device__ __forceinline__ int apply_tf(uint32_t f, int c) {
   return (int)((f >> (2 * (c + 1))) & 3u) - 1;
@@ -296,226 +295,6 @@ __device__ __forceinline__ uint32_t word_tf(uint32_t y, int g) {
   }
   return f;
 }
-
-template <int P>
-__global__ void __launch_bounds__(kRecThreads)
-k_crt_recompose(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
-                const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
-                int32_t* __restrict__ out_sizes, int words_per_thread) {
-  extern __shared__ uint32_t sm[];
-  __shared__ uint32_t s_post[P], s_postq[P];
-  __shared__ uint32_t s_warp_tf[kRecThreads / 32];
-  __shared__ int s_warp_hi[kRecThreads / 32];
-  __shared__ int s_hi_prev, s_carry;
-  __shared__ uint32_t s_top;
-  __shared__ int s_first_nz, s_last_nz, s_last_no;
-
-  const InvDesc d = descs[idx[blockIdx.x]];
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int wid = tid >> 5;
-  const int bs = blockDim.x;
-  const int N = 1 << d.lgN;
-  const int64_t r = d.r;
-  const int64_t W = d.out_words;
-  const int64_t ncoef = d.ncoef;
-  uint32_t* o = out + d.out_word;
-  const int64_t TW = (int64_t)bs * words_per_thread;
-
-  if (tid < P) {
-    const uint32_t p = c_primes[tid].p;
-    // N^{-1} mod p = p - (p-1)/N since p = 1 mod N; the contraction left a
-    // Montgomery factor 2^-32, so scale by 2^32 N^{-1} = redc(2^64 N^{-1}).
-    const uint32_t ninv = p - ((p - 1) >> d.lgN);
-    const uint32_t post = redc((uint64_t)c_primes[tid].r2 * ninv, p, c_primes[tid].pinv);
-    s_post[tid] = post;
-    s_postq[tid] = shoup_of(post, p);
-  }
-  if (tid == 0) {
-    s_hi_prev = 0;
-    s_carry = 0;
-    s_top = 0;
-    s_first_nz = 0x7fffffff;
-    s_last_nz = -1;
-    s_last_no = -1;
-  }
-  __syncthreads();
-
-  uint32_t* sU = sm;  // [cmax][P] words, then sign bytes
-  int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
-
-  for (int64_t w0 = 0; w0 < W; w0 += TW) {
-    // coefficients overlapping words [w0, w0 + TW), borrow landings included
-    int64_t lo_i = (32 * w0 - 32 * (int64_t)P + r - 1) / r;  // ceil, may be < 0
-    if (32 * w0 - 32 * (int64_t)P < 0) lo_i = 0;
-    int64_t hi_i = (32 * (w0 + TW) - 1) / r;
-    if (hi_i > ncoef - 1) hi_i = ncoef - 1;
-    const int64_t ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
-    uint8_t* sS = reinterpret_cast<uint8_t*>(sU + (size_t)ncf * P);
-
-    // ---- Garner for every coefficient of the tile ----
-    for (int64_t c = tid; c < ncf; c += bs) {
-      const int64_t ic = lo_i + c;
-      uint32_t v[P];
-#pragma unroll
-      for (int q = 0; q < P; ++q) {
-        const uint32_t p = c_primes[q].p;
-        uint32_t x = res[d.res_off + (uint64_t)q * N + ic];
-        x = mul_shoup(x, s_post[q], s_postq[q], p);
-        if (q == 0) {
-          v[0] = x;
-        } else {
-          // t = (v_0 + v_1 p_0 + ... + v_{q-1} p_0...p_{q-2}) mod p_q (Horner)
-          uint32_t t = v[q - 1] >= p ? v[q - 1] - p : v[q - 1];
-#pragma unroll
-          for (int a = q - 2; a >= 0; --a) {
-            uint32_t va = v[a] >= p ? v[a] - p : v[a];
-            t = add_mod(mul_shoup(t, c_crt.pmod[q][a], c_crt.pmodq[q][a], p), va, p);
-          }
-          v[q] = mul_shoup(sub_mod(x, t, p), c_crt.inv[q], c_crt.invq[q], p);
-        }
-      }
-      // X = v_{P-1}; X = X p_i + v_i for i = P-2 .. 0
-      uint32_t X[P];
-#pragma unroll
-      for (int q = 0; q < P; ++q) X[q] = 0;
-      X[0] = v[P - 1];
-#pragma unroll
-      for (int i = P - 2; i >= 0; --i) {
-        const uint32_t pi = c_primes[i].p;
-        uint64_t cy = v[i];
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-          const uint64_t t = (uint64_t)X[q] * pi + cy;
-          X[q] = (uint32_t)t;
-          cy = t >> 32;
-        }
-      }
-      // symmetric residue: X > M/2  ->  X - M (two's complement, P words)
-      bool gt = false, decided = false;
-#pragma unroll
-      for (int q = P - 1; q >= 0; --q) {
-        const uint32_t hq = c_crt.Mhalf[P][q];
-        if (!decided && X[q] != hq) {
-          gt = X[q] > hq;
-          decided = true;
-        }
-      }
-      if (gt) {
-        uint32_t br = 0;
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-          const uint64_t t = (uint64_t)X[q] - c_crt.M[P][q] - br;
-          X[q] = (uint32_t)t;
-          br = (uint32_t)(t >> 63);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < P; ++q) sU[c * P + q] = X[q];
-      sS[c] = gt ? 1 : 0;
-    }
-    __syncthreads();
-
-    // ---- word sums, carry normalisation and the carry scan ----
-    for (int s = 0; s < words_per_thread; ++s) {
-      const int64_t w = w0 + (int64_t)s * bs + tid;
-      const bool active = w < W && w < w0 + TW;
-      int64_t sw = 0;
-      if (active) {
-        int64_t ia = (32 * w - 32 * (int64_t)P + r - 1) / r;
-        if (32 * w - 32 * (int64_t)P < 0) ia = 0;
-        if (ia < lo_i) ia = lo_i;
-        int64_t ib = (32 * w + 31) / r;
-        if (ib > hi_i) ib = hi_i;
-        for (int64_t i = ia; i <= ib; ++i) {
-          const int64_t c = i - lo_i;
-          const int64_t bi = i * r;
-          const int64_t dd = 32 * w - bi;  // bit of U_i that lands on bit 0 of w
-          const uint32_t* U = sU + c * P;
-          uint32_t slice;
-          if (dd < 0) {
-            slice = U[0] << (uint32_t)(-dd);
-          } else {
-            const int64_t q = dd >> 5;
-            const uint32_t sh = (uint32_t)(dd & 31);
-            const uint32_t lo = q < P ? U[q] : 0u;
-            const uint32_t hi = q + 1 < P ? U[q + 1] : 0u;
-            slice = __funnelshift_r(lo, hi, sh);
-          }
-          sw += slice;
-          if (sS[c] && (bi >> 5) + P == w) sw -= (int64_t)1 << (bi & 31);
-        }
-      }
-      const uint32_t lo = (uint32_t)sw;
-      const int hi = (int)(sw >> 32);
-      // hi of word w-1
-      int hprev = __shfl_up_sync(0xffffffffu, hi, 1);
-      if (lane == 31) s_warp_hi[wid] = hi;
-      __syncthreads();
-      if (lane == 0) hprev = (wid == 0) ? s_hi_prev : s_warp_hi[wid - 1];
-      const int64_t z = (int64_t)lo + hprev;
-      const uint32_t y = (uint32_t)z;
-      const int g = (int)(z >> 32);
-      uint32_t f = active ? word_tf(y, g) : kTfIdentity;
-      // inclusive warp scan of transfer functions
-      uint32_t inc = f;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, off);
-        if (lane >= off) inc = compose_tf(inc, u);
-      }
-      if (lane == 31) s_warp_tf[wid] = inc;
-      uint32_t exc = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) exc = kTfIdentity;
-      __syncthreads();
-      // prefix of earlier warps
-      uint32_t wp = kTfIdentity;
-      for (int q = 0; q < wid; ++q) wp = compose_tf(s_warp_tf[q], wp);
-      const int cin_block = s_carry;
-      const int cin = apply_tf(compose_tf(exc, wp), cin_block);
-      if (active) {
-        const uint32_t F = y + (uint32_t)cin;
-        o[w] = F;
-        if (F != 0u) {
-          if ((int)w < first_nz) first_nz = (int)w;
-          if ((int)w > last_nz) last_nz = (int)w;
-        }
-        if (F != 0xffffffffu && (int)w > last_no) last_no = (int)w;
-        if (w == W - 1) s_top = F;
-      }
-      __syncthreads();
-      if (tid == bs - 1) {
-        uint32_t tot = kTfIdentity;
-        for (int q = 0; q < bs / 32; ++q) tot = compose_tf(s_warp_tf[q], tot);
-        s_carry = apply_tf(tot, cin_block);
-        s_hi_prev = hi;
-      }
-      __syncthreads();
-    }
-  }
-
-  atomicMin(&s_first_nz, first_nz);
-  atomicMax(&s_last_nz, last_nz);
-  atomicMax(&s_last_no, last_no);
-  __syncthreads();
-  const bool negative = W > 0 && (s_top >> 31);
-  int top;
-  if (negative) {
-    const int zf = s_first_nz;  // exists: a negative value is nonzero
-    for (int64_t w = zf + tid; w < W; w += bs) {
-      const uint32_t F = o[w];
-      o[w] = (w == zf) ? (0u - F) : ~F;
-    }
-    top = s_last_no > zf ? s_last_no : zf;
-  } else {
-    top = s_last_nz;
-  }
-  if (tid == 0) {
-    const int limbs = top >= 0 ? top / 2 + 1 : 0;
-    out_sizes[d.entry] = negative ? -limbs : limbs;
-  }
-}
-
 
 // ---------------------------------------------------------------------------
 // Split + forward NTT, register-blocked (lgN >= 3).
@@ -670,6 +449,209 @@ k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// CRT + recompose, one warp per output entry (no block barriers).
+//
+// Same arithmetic as k_crt_recompose: Garner to the symmetric P-word value
+// U_i - s_i 2^(32P) of each coefficient, per-word gathered sums, carries
+// normalised into {-1, 0, 1}.  The ripple is resolved per 32-word step: when
+// no word of the step is 0 or all-ones (a carry can only pass through such a
+// word), word w's incoming carry is just the generated carry g_{w-1}; only
+// otherwise does the warp run the prefix scan of transfer functions.  The
+// post-scale 2^32 N^{-1} mod p comes precomputed from constant memory.
+// ---------------------------------------------------------------------------
+constexpr int kCrtWarps = 4;       // entries per CTA
+constexpr int kCrtSteps = 8;       // 32-word steps per tile
+constexpr int kCrtTileWords = 32 * kCrtSteps;
+
+template <int P>
+__device__ __forceinline__ bool garner_coeff(const uint32_t* __restrict__ res, uint64_t res_off,
+                                             int lgN, int64_t ic, uint32_t (&X)[P]) {
+  const uint64_t N = (uint64_t)1 << lgN;
+  uint32_t v[P];
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    const uint32_t p = c_primes[q].p;
+    uint32_t x = __ldg(res + res_off + (uint64_t)q * N + (uint64_t)ic);
+    x = mul_shoup(x, c_crt.post[lgN][q], c_crt.postq[lgN][q], p);
+    if (q == 0) {
+      v[0] = x;
+    } else {
+      uint32_t t = v[q - 1] >= p ? v[q - 1] - p : v[q - 1];
+#pragma unroll
+      for (int a = q - 2; a >= 0; --a) {
+        const uint32_t va = v[a] >= p ? v[a] - p : v[a];
+        t = add_mod(mul_shoup(t, c_crt.pmod[q][a], c_crt.pmodq[q][a], p), va, p);
+      }
+      v[q] = mul_shoup(sub_mod(x, t, p), c_crt.inv[q], c_crt.invq[q], p);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) X[q] = 0;
+  X[0] = v[P - 1];
+#pragma unroll
+  for (int i = P - 2; i >= 0; --i) {
+    const uint32_t pi = c_primes[i].p;
+    uint64_t cy = v[i];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const uint64_t t = (uint64_t)X[q] * pi + cy;
+      X[q] = (uint32_t)t;
+      cy = t >> 32;
+    }
+  }
+  bool gt = false, decided = false;
+#pragma unroll
+  for (int q = P - 1; q >= 0; --q) {
+    const uint32_t hq = c_crt.Mhalf[P][q];
+    if (!decided && X[q] != hq) {
+      gt = X[q] > hq;
+      decided = true;
+    }
+  }
+  if (gt) {
+    uint32_t br = 0;
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+      const uint64_t t = (uint64_t)X[q] - c_crt.M[P][q] - br;
+      X[q] = (uint32_t)t;
+      br = (uint32_t)(t >> 63);
+    }
+  }
+  return gt;
+}
+
+template <int P>
+__global__ void __launch_bounds__(32 * kCrtWarps)
+k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
+           const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
+           int32_t* __restrict__ out_sizes, int cmax) {
+  extern __shared__ uint32_t sm[];
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int slot = blockIdx.x * kCrtWarps + warp;
+  if (slot >= count) return;  // whole warp; no block-wide barrier below
+  const InvDesc d = descs[idx[slot]];
+  const int64_t r = d.r;
+  const int64_t W = d.out_words;
+  const int64_t ncoef = d.ncoef;
+  uint32_t* o = out + d.out_word;
+  const int per_warp_words = cmax * P + (cmax + 3) / 4;
+  uint32_t* sU = sm + warp * per_warp_words;
+  uint8_t* sS = reinterpret_cast<uint8_t*>(sU + cmax * P);
+
+  int hi_prev = 0, carry = 0;
+  int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
+  uint32_t topval = 0;
+  for (int64_t w0 = 0; w0 < W; w0 += kCrtTileWords) {
+    int64_t lo_i = 0;
+    if (32 * w0 - 32 * (int64_t)P > 0) lo_i = (32 * w0 - 32 * (int64_t)P + r - 1) / r;
+    int64_t hi_i = (32 * (w0 + kCrtTileWords) - 1) / r;
+    if (hi_i > ncoef - 1) hi_i = ncoef - 1;
+    const int64_t ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
+    for (int64_t c = lane; c < ncf; c += 32) {
+      uint32_t X[P];
+      const bool neg = garner_coeff<P>(res, d.res_off, d.lgN, lo_i + c, X);
+#pragma unroll
+      for (int q = 0; q < P; ++q) sU[c * P + q] = X[q];
+      sS[c] = neg ? 1 : 0;
+    }
+    __syncwarp();
+    for (int st = 0; st < kCrtSteps; ++st) {
+      const int64_t w = w0 + st * 32 + lane;
+      const bool active = w < W;
+      int64_t sw = 0;
+      if (active) {
+        int64_t ia = lo_i;
+        if (32 * w - 32 * (int64_t)P > 0) {
+          const int64_t t = (32 * w - 32 * (int64_t)P + r - 1) / r;
+          if (t > ia) ia = t;
+        }
+        int64_t ib = (32 * w + 31) / r;
+        if (ib > hi_i) ib = hi_i;
+        for (int64_t i = ia; i <= ib; ++i) {
+          const int64_t c = i - lo_i;
+          const int64_t bi = i * r;
+          const int64_t dd = 32 * w - bi;
+          const uint32_t* U = sU + c * P;
+          uint32_t slice;
+          if (dd < 0) {
+            slice = U[0] << (uint32_t)(-dd);
+          } else {
+            const int64_t q = dd >> 5;
+            const uint32_t sh = (uint32_t)(dd & 31);
+            const uint32_t lo = q < P ? U[q] : 0u;
+            const uint32_t hi = q + 1 < P ? U[q + 1] : 0u;
+            slice = __funnelshift_r(lo, hi, sh);
+          }
+          sw += slice;
+          if (sS[c] && (bi >> 5) + P == w) sw -= (int64_t)1 << (bi & 31);
+        }
+      }
+      const int hi = active ? (int)(sw >> 32) : 0;
+      int hprev = __shfl_up_sync(FULL, hi, 1);
+      if (lane == 0) hprev = hi_prev;
+      const int64_t z = (int64_t)(uint32_t)sw + hprev;
+      const uint32_t y = (uint32_t)z;
+      const int g = active ? (int)(z >> 32) : 0;
+      const bool prop = active && (y == 0u || y == 0xffffffffu);
+      int cin, cout;
+      if (__any_sync(FULL, prop)) {
+        const uint32_t f = active ? word_tf(y, g) : kTfIdentity;
+        uint32_t inc = f;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const uint32_t u = __shfl_up_sync(FULL, inc, off);
+          if (lane >= off) inc = compose_tf(inc, u);
+        }
+        uint32_t exc = __shfl_up_sync(FULL, inc, 1);
+        if (lane == 0) exc = kTfIdentity;
+        cin = apply_tf(exc, carry);
+        cout = apply_tf(__shfl_sync(FULL, inc, 31), carry);
+      } else {
+        cin = __shfl_up_sync(FULL, g, 1);
+        if (lane == 0) cin = carry;
+        cout = __shfl_sync(FULL, g, 31);
+      }
+      if (active) {
+        const uint32_t F = y + (uint32_t)cin;
+        o[w] = F;
+        if (F != 0u) {
+          if ((int)w < first_nz) first_nz = (int)w;
+          last_nz = (int)w;
+        }
+        if (F != 0xffffffffu) last_no = (int)w;
+        if (w == W - 1) topval = F;
+      }
+      hi_prev = __shfl_sync(FULL, hi, 31);
+      carry = cout;
+    }
+    __syncwarp();
+  }
+  first_nz = __reduce_min_sync(FULL, first_nz);
+  last_nz = __reduce_max_sync(FULL, last_nz);
+  last_no = __reduce_max_sync(FULL, last_no);
+  topval = __reduce_or_sync(FULL, topval);
+  const bool negative = W > 0 && (topval >> 31);
+  int top;
+  if (negative) {
+    const int zf = first_nz;
+    for (int64_t w = zf + lane; w < W; w += 32) {
+      const uint32_t F = o[w];
+      o[w] = (w == zf) ? (0u - F) : ~F;
+    }
+    top = last_no > zf ? last_no : zf;
+  } else {
+    top = last_nz;
+  }
+  if (lane == 0) {
+    const int limbs = top >= 0 ? top / 2 + 1 : 0;
+    out_sizes[d.entry] = negative ? -limbs : limbs;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -783,46 +765,50 @@ cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, in
 }
 
 int contract_block_freqs() { return kContractThreads; }
-int recompose_threads() { return kRecThreads; }
 
 template <int P>
-static cudaError_t launch_rec_t(const InvDesc* descs, const uint32_t* idx, int count,
-                                const uint32_t* res, uint32_t* out, int32_t* sizes,
-                                int words_per_thread, size_t smem, cudaStream_t st) {
+static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int count,
+                                const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
+                                cudaStream_t st) {
+  const int cmax = (int)((32 * (int64_t)kCrtTileWords + 32 * P) / rmin + 3);
+  const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P + (cmax + 3) / 4);
+  const size_t smem = per_warp * kCrtWarps;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_crt_recompose<P>,
+    cudaError_t e = cudaFuncSetAttribute(k_crt_warp<P>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_crt_recompose<P><<<count, kRecThreads, smem, st>>>(descs, idx, res, out, sizes,
-                                                       words_per_thread);
+  const int grid = (count + kCrtWarps - 1) / kCrtWarps;
+  k_crt_warp<P><<<grid, 32 * kCrtWarps, smem, st>>>(descs, idx, count, res, out, sizes, cmax);
   return cudaGetLastError();
 }
 
 cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int count, int P,
-                                 const uint32_t* res, uint32_t* out, int32_t* sizes,
-                                 int words_per_thread, size_t smem, cudaStream_t st) {
+                                 const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
+                                 cudaStream_t st) {
   if (count == 0) return cudaSuccess;
+  if (rmin < 1) return cudaErrorInvalidValue;
   switch (P) {
-#define MPZMM_REC_CASE(PP) \
+#define MPZMM_CRT_CASE(PP) \
   case PP:                 \
-    return launch_rec_t<PP>(descs, idx, count, res, out, sizes, words_per_thread, smem, st);
-    MPZMM_REC_CASE(2)
-    MPZMM_REC_CASE(3)
-    MPZMM_REC_CASE(4)
-    MPZMM_REC_CASE(5)
-    MPZMM_REC_CASE(6)
-    MPZMM_REC_CASE(7)
-    MPZMM_REC_CASE(8)
-    MPZMM_REC_CASE(9)
-    MPZMM_REC_CASE(10)
-    MPZMM_REC_CASE(11)
-    MPZMM_REC_CASE(12)
-    MPZMM_REC_CASE(13)
-    MPZMM_REC_CASE(14)
-    MPZMM_REC_CASE(15)
-    MPZMM_REC_CASE(16)
-#undef MPZMM_REC_CASE
+    return launch_crt_t<PP>(descs, idx, count, res, out, sizes, rmin, st);
+    MPZMM_CRT_CASE(2)
+    MPZMM_CRT_CASE(3)
+    MPZMM_CRT_CASE(4)
+    MPZMM_CRT_CASE(5)
+    MPZMM_CRT_CASE(6)
+    MPZMM_CRT_CASE(7)
+    MPZMM_CRT_CASE(8)
+    MPZMM_CRT_CASE(9)
+    MPZMM_CRT_CASE(10)
+    MPZMM_CRT_CASE(11)
+    MPZMM_CRT_CASE(12)
+    MPZMM_CRT_CASE(13)
+    MPZMM_CRT_CASE(14)
+    MPZMM_CRT_CASE(15)
+    MPZMM_CRT_CASE(16)
+#undef MPZMM_CRT_CASE
     default:
       return cudaErrorInvalidValue;
   }

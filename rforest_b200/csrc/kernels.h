@@ -25,10 +25,10 @@ cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, in
                             uint32_t* res, cudaStream_t st);
 int contract_block_freqs();
 
-// CRT + recompose + sign for `count` output entries with P primes.
+// CRT + recompose + sign for `count` output entries with P primes; rmin is
+// the narrowest coefficient width among them (it sizes the shared scratch).
 cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int count, int P,
-                                 const uint32_t* res, uint32_t* out, int32_t* sizes,
-                                 int words_per_thread, size_t smem, cudaStream_t st);
-int recompose_threads();
+                                 const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
+                                 cudaStream_t st);
 
 }  // namespace mpzmm

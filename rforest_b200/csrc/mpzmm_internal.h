@@ -46,6 +46,11 @@ struct CrtConst {
   uint32_t M[kMaxPrimes + 1][kMaxCrtWords];
   uint32_t Mhalf[kMaxPrimes + 1][kMaxCrtWords];
   int Mwords[kMaxPrimes + 1];              // words of M_P
+  // scale applied to a CRT input residue of a 2^lgN-point transform:
+  // 2^32 N^{-1} mod p_j (removes the contraction's Montgomery factor and the
+  // inverse transform's factor N), with Shoup companions
+  uint32_t post[kMaxLgN + 1][kMaxPrimes];
+  uint32_t postq[kMaxLgN + 1][kMaxPrimes];
 };
 
 // One polynomial (one matrix entry) of the forward transform.

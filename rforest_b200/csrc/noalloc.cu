@@ -223,20 +223,6 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   const ContractItem* ditems = reinterpret_cast<const ContractItem*>(dd + off_items);
   const uint32_t* didx = reinterpret_cast<const uint32_t*>(dd + off_idx);
 
-  // CRT window for this r and P (same rule as the batch engine)
-  const int rt = recompose_threads();
-  int wpt = 1;
-  size_t smem = 0;
-  for (int S : {8, 4, 2, 1}) {
-    const int64_t TW = (int64_t)rt * S;
-    const int64_t cmax = (32 * TW + 32 * P) / r + 3;
-    const int64_t bytes = cmax * (4 * P + 1);
-    if (bytes <= 96 * 1024 || S == 1) {
-      wpt = S;
-      smem = (size_t)((bytes + 15) & ~15LL);
-      break;
-    }
-  }
   if ((e = launch_split_fwd(dfwd, didx, (int)na, P, lgN, d_a_limbs, dres, ds->twf, s, r)) !=
           cudaSuccess ||
       (e = launch_split_fwd(dfwd, didx + na, (int)nb, P, lgN, d_b_limbs, dres, ds->twf, s, r)) !=
@@ -245,7 +231,7 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
       (e = launch_inv_ntt(dinv, didx + na + nb, (int)nc, P, lgN, dres, ds->twi, s)) !=
           cudaSuccess ||
       (e = launch_crt_recompose(dinv, didx + na + nb, (int)nc, P, dres,
-                                reinterpret_cast<uint32_t*>(d_c_limbs), d_c_sizes, wpt, smem, s)) !=
+                                reinterpret_cast<uint32_t*>(d_c_limbs), d_c_sizes, r, s)) !=
           cudaSuccess)
     return cufail(e, "mpzmm_matmul_noalloc launch");
   return kOk;

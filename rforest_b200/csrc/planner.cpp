@@ -151,6 +151,14 @@ void build(Moduli& M) {
     M.crt.inv[i] = iv;
     M.crt.invq[i] = shoup(iv, p);
   }
+  for (int lg = 0; lg <= kMaxLgN; ++lg)
+    for (int j = 0; j < kMaxPrimes; ++j) {
+      const uint32_t p = M.p[j];
+      const uint64_t ninv = powmod((uint64_t)1 << lg, p - 2, p);
+      const uint32_t post = (uint32_t)((((uint64_t)1 << 32) % p) * ninv % p);
+      M.crt.post[lg][j] = post;
+      M.crt.postq[lg][j] = shoup(post, p);
+    }
   std::vector<uint32_t> acc{1};
   for (int P = 1; P <= kMaxPrimes; ++P) {
     mul_small(acc, M.p[P - 1]);
