@@ -1,6 +1,7 @@
 // Batch engine (see engine.h).
 #include "engine.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -357,15 +358,60 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   if (out_entry > 0x7fffffffULL) return set_error(kErrTooLarge, "too many output entries");
 
   // launch groups and the shared index array
-  for (auto& kv : fwdg) fwd_groups_.push_back(std::move(kv.second));
-  for (auto& kv : invg) inv_groups_.push_back(std::move(kv.second));
+  // Transforms: size classes with lgN >= 3 are merged into one launch per
+  // kernel variant (team or not, digits D), CTA work items carrying the
+  // class; the largest classes come first so the long CTAs start early.
+  auto batch_classes = [&](std::map<std::pair<int, int>, Group>& classes, bool fwd,
+                           std::vector<Group>& out) {
+    std::map<std::pair<int, int>, Group> var;
+    for (auto& kv : classes) {
+      Group& g = kv.second;
+      const int D = fwd ? (g.max_r + 29) / 30 : 0;
+      if (g.lgN < 3 || D > 7) {
+        out.push_back(std::move(g));  // radix-2 path
+        continue;
+      }
+      const bool team = ((int64_t)1 << g.lgN) <= (int64_t)fwd_team_points();
+      Group& v = var[{team ? 1 : 0, D}];
+      v.batched = true;
+      v.team = team;
+      v.D = D;
+      if (g.lgN > v.max_lgN) v.max_lgN = g.lgN;
+      const size_t G = team ? (size_t)(fwd_team_points() >> g.lgN) : 1;
+      for (size_t i = 0; i < g.idx.size(); i += G) {
+        const size_t cnt = (g.idx.size() - i) < G ? (g.idx.size() - i) : G;
+        CtaItem it;
+        it.first = (uint32_t)idx_all_.size();
+        it.count = (uint16_t)cnt;
+        it.lgN = (uint8_t)g.lgN;
+        it.P = (uint8_t)g.P;
+        idx_all_.insert(idx_all_.end(), g.idx.begin() + i, g.idx.begin() + i + cnt);
+        v.items.push_back(it);
+      }
+    }
+    for (auto& kv : var) {
+      Group& v = kv.second;
+      std::stable_sort(v.items.begin(), v.items.end(),
+                       [](const CtaItem& a, const CtaItem& b) { return a.lgN > b.lgN; });
+      v.item_off = (uint32_t)cta_items_.size();
+      cta_items_.insert(cta_items_.end(), v.items.begin(), v.items.end());
+      out.push_back(std::move(v));
+    }
+  };
+  batch_classes(fwdg, true, fwd_groups_);
+  batch_classes(invg, false, inv_groups_);
   for (auto& kv : recg) {
     Group g = std::move(kv.second);
     g.max_r = (int)rec_min_r[g.P];  // narrowest r: sizes the CRT kernel's scratch
+    // longest entries first (the warp that gets one works longest)
+    std::stable_sort(g.idx.begin(), g.idx.end(), [&](uint32_t a, uint32_t b) {
+      return inv_[a].out_words > inv_[b].out_words;
+    });
     rec_groups_.push_back(std::move(g));
   }
   for (auto* gs : {&fwd_groups_, &inv_groups_, &rec_groups_})
     for (auto& g : *gs) {
+      if (g.batched) continue;
       g.idx_off = (uint32_t)idx_all_.size();
       idx_all_.insert(idx_all_.end(), g.idx.begin(), g.idx.end());
     }
@@ -380,7 +426,8 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   off_pd_ = align16(off_inv_ + inv_.size() * sizeof(InvDesc));
   off_items_ = align16(off_pd_ + pd_.size() * sizeof(ProdDesc));
   off_idx_ = align16(off_items_ + items_.size() * sizeof(ContractItem));
-  desc_bytes_ = align16(off_idx_ + idx_all_.size() * sizeof(uint32_t));
+  off_cta_ = align16(off_idx_ + idx_all_.size() * sizeof(uint32_t));
+  desc_bytes_ = align16(off_cta_ + cta_items_.size() * sizeof(CtaItem));
   ws_ = ws ? ws : &own_;
   int st = ws_->reserve(n_limbs_, n_res_, n_out_words_, outs_.size(), desc_bytes_);
   if (st) return st;
@@ -392,11 +439,14 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     std::memcpy(hd + off_items_, items_.data(), items_.size() * sizeof(ContractItem));
   if (!idx_all_.empty())
     std::memcpy(hd + off_idx_, idx_all_.data(), idx_all_.size() * sizeof(uint32_t));
+  if (!cta_items_.empty())
+    std::memcpy(hd + off_cta_, cta_items_.data(), cta_items_.size() * sizeof(CtaItem));
   d_fwd_ = reinterpret_cast<FwdDesc*>(ws_->d_desc + off_fwd_);
   d_inv_ = reinterpret_cast<InvDesc*>(ws_->d_desc + off_inv_);
   d_pd_ = reinterpret_cast<ProdDesc*>(ws_->d_desc + off_pd_);
   d_items_ = reinterpret_cast<ContractItem*>(ws_->d_desc + off_items_);
   d_idx_ = reinterpret_cast<uint32_t*>(ws_->d_desc + off_idx_);
+  d_cta_ = reinterpret_cast<CtaItem*>(ws_->d_desc + off_cta_);
   launches_ = (int64_t)fwd_groups_.size() + (items_.empty() ? 0 : 1) +
               (int64_t)inv_groups_.size() + (int64_t)rec_groups_.size();
   built_ = true;
@@ -452,18 +502,30 @@ int Plan::execute(cudaStream_t st) {
     }
     CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
   }
-  for (const Group& g : fwd_groups_)
-    CU(launch_split_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN,
-                        ws_->d_limbs, ws_->d_res, ctx.d_twf, st, g.max_r),
-       "split+forward NTT launch");
+  for (const Group& g : fwd_groups_) {
+    if (g.batched)
+      CU(launch_fwd_items(d_fwd_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.D, g.team,
+                          g.max_lgN, ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
+         "split+forward NTT launch");
+    else
+      CU(launch_split_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN,
+                          ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
+         "split+forward NTT launch");
+  }
   if (timing_) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
   if (timing_) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
-  for (const Group& g : inv_groups_)
-    CU(launch_inv_ntt(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN,
-                      ws_->d_res, ctx.d_twi, st),
-       "inverse NTT launch");
+  for (const Group& g : inv_groups_) {
+    if (g.batched)
+      CU(launch_inv_items(d_inv_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.team,
+                          g.max_lgN, ws_->d_res, ctx.d_twi, st),
+         "inverse NTT launch");
+    else
+      CU(launch_inv_ntt(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN, ws_->d_res,
+                        ctx.d_twi, st),
+         "inverse NTT launch");
+  }
   if (timing_) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
   for (const Group& g : rec_groups_)
     CU(launch_crt_recompose(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, ws_->d_res,

@@ -125,6 +125,13 @@ class Plan {
     int max_r = 0;         // split: widest coefficient; CRT: narrowest coefficient
     uint32_t idx_off = 0;  // into the device index array
     std::vector<uint32_t> idx;
+    // batched transform launch (several size classes, CTA work items)
+    bool batched = false;
+    bool team = false;
+    int D = 0;
+    int max_lgN = 0;
+    std::vector<CtaItem> items;
+    uint32_t item_off = 0;
   };
 
   std::vector<ProductSpec> prods_;
@@ -135,6 +142,7 @@ class Plan {
   std::vector<ContractItem> items_;
   std::vector<Group> fwd_groups_, inv_groups_, rec_groups_;
   std::vector<uint32_t> idx_all_;
+  std::vector<CtaItem> cta_items_;
   std::vector<OutRef> outs_;          // flattened output references
   std::vector<int64_t> out_word_off_; // per output entry (words)
   std::vector<uint8_t> zero_prod_;    // product is identically zero
@@ -145,7 +153,9 @@ class Plan {
   Workspace own_;
   Workspace* ws_ = nullptr;
   // descriptor blob: offsets of each section (bytes) and its size
-  size_t off_fwd_ = 0, off_inv_ = 0, off_pd_ = 0, off_items_ = 0, off_idx_ = 0, desc_bytes_ = 0;
+  size_t off_fwd_ = 0, off_inv_ = 0, off_pd_ = 0, off_items_ = 0, off_idx_ = 0, off_cta_ = 0,
+         desc_bytes_ = 0;
+  CtaItem* d_cta_ = nullptr;
   FwdDesc* d_fwd_ = nullptr;
   InvDesc* d_inv_ = nullptr;
   ProdDesc* d_pd_ = nullptr;

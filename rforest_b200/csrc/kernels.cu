@@ -5,10 +5,10 @@
 //   k_contract       per frequency h and prime: C[h] = A[h] B[h] mod p on
 //                    CUDA cores (64-bit lazy accumulation, Montgomery fold)
 //   k_inv_ntt        inverse NTT in shared memory (one CTA per (entry, prime))
-//   k_crt_recompose  Garner CRT to signed multi-word coefficients, then
-//                    sum_i c_i 2^(i r) as a carry-lookahead prefix scan over
-//                    32-bit output words, sign + negation + normalisation
-//                    (one CTA per output entry)
+//   k_crt_warp       explicit CRT to signed multi-word coefficients, then
+//                    sum_i c_i 2^(i r) with carries resolved by a
+//                    carry-lookahead prefix scan over 32-bit output words,
+//                    sign + negation + normalisation (one warp per entry)
 //
 // Reference counterparts: split/reduce src/lib/split_reduce.c:15-66,
 // NTTs src/lib/mpnfft.c:354-432, contraction src/lib/mpnfft.c:559-651,
@@ -253,20 +253,21 @@ k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// CRT + recompose + sign + normalise.  One CTA per output entry.
+// CRT + recompose + sign + normalise: shared pieces.
 //
-// Coefficient i of the entry is recovered by Garner's algorithm as the
-// symmetric residue X_i in (-M/2, M/2], M = p_0...p_{P-1}, and written as
-// X_i = U_i - s_i 2^(32P) with U_i the P-word two's complement and s_i its
-// sign bit.  The entry is sum_i X_i 2^(i r) mod 2^(32 W).  Output word w
-// gathers its local sum
+// Coefficient i of an output entry is recovered as the symmetric residue
+// X_i in (-M/4, M/4), M = p_0...p_{P-1}, written as X_i = U_i - s_i 2^(32P)
+// with U_i the P-word two's complement and s_i its sign bit.  The entry is
+// sum_i X_i 2^(i r) mod 2^(32 W).  Output word w gathers its local sum
 //      s_w = sum_i slice_w(U_i 2^(i r)) - sum_i s_i [borrow of i lands in w]
 // (a small signed 64-bit value), then s_w = lo_w + 2^32 hi_w is rewritten as
 // words y_w with carries g_w in {-1,0,1}; the remaining carry ripple is a
 // prefix scan whose element is the word's transfer function
 // {-1,0,1} -> {-1,0,1}, composed associatively.  This is the parallel form
 // of the reference's serial borrow chain (src/lib/recompose.c:43-87) and of
-// its chunk fix-up (src/lib/crt_recompose.c:101-153).
+// its chunk fix-up (src/lib/crt_recompose.c:101-153); the reference's CRT is
+// Garner's (src/lib/crt.c:11-94), the explicit form here needs O(P) modular
+// products instead of O(P^2).
 // ---------------------------------------------------------------------------
 
 __device__ __forceinline__ int apply_tf(uint32_t f, int c) {
@@ -341,17 +342,18 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
 
 template <int D, bool TEAM>
 __global__ void __launch_bounds__(kFwdThreads)
-k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
-       int lgN, int P, const uint64_t* __restrict__ limbs, uint32_t* __restrict__ res,
-       const uint2* __restrict__ twf) {
+k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
+       const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
+       uint32_t* __restrict__ res, const uint2* __restrict__ twf) {
   extern __shared__ uint32_t sm[];
+  const CtaItem item = items[blockIdx.x];
+  const int lgN = item.lgN;
+  const int P = item.P;
   const int N = 1 << lgN;
   const int TS = TEAM ? (N >> 3) : kFwdThreads;  // threads per entry
   const int team = TEAM ? (int)threadIdx.x / TS : 0;
   const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
-  const int G = TEAM ? kFwdThreads / TS : 1;
-  const int slot = blockIdx.x * G + team;
-  const bool valid = slot < count;
+  const bool valid = team < (int)item.count;
   uint32_t* s = sm + team * (N + (N >> 5));
   FwdDesc d;
   d.limb_off = 0;
@@ -359,7 +361,7 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int 
   d.size = 0;
   d.r = 1;
   d.ncoef = 0;
-  if (valid) d = descs[idx[slot]];
+  if (valid) d = descs[idx[item.first + team]];
   const uint64_t nw = 2ull * (uint64_t)(d.size < 0 ? -d.size : d.size);
   const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
   const bool neg = d.size < 0;
@@ -410,18 +412,20 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int 
 // Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
 template <bool TEAM>
 __global__ void __launch_bounds__(kFwdThreads)
-k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count, int lgN,
-       int P, uint32_t* __restrict__ res, const uint2* __restrict__ twi) {
+k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
+       const CtaItem* __restrict__ items, uint32_t* __restrict__ res,
+       const uint2* __restrict__ twi) {
   extern __shared__ uint32_t sm[];
+  const CtaItem item = items[blockIdx.x];
+  const int lgN = item.lgN;
+  const int P = item.P;
   const int N = 1 << lgN;
   const int TS = TEAM ? (N >> 3) : kFwdThreads;
   const int team = TEAM ? (int)threadIdx.x / TS : 0;
   const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
-  const int G = TEAM ? kFwdThreads / TS : 1;
-  const int slot = blockIdx.x * G + team;
-  const bool valid = slot < count;
+  const bool valid = team < (int)item.count;
   uint32_t* s = sm + team * (N + (N >> 5));
-  const uint64_t off = valid ? descs[idx[slot]].res_off : 0;
+  const uint64_t off = valid ? descs[idx[item.first + team]].res_off : 0;
   const int last_s0 = ((lgN - 1) / 3) * 3;  // start of the last forward pass
   for (int j = 0; j < P; ++j) {
     const uint32_t p = c_primes[j].p;
@@ -453,73 +457,53 @@ k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int 
 // ---------------------------------------------------------------------------
 // CRT + recompose, one warp per output entry (no block barriers).
 //
-// Same arithmetic as k_crt_recompose: Garner to the symmetric P-word value
-// U_i - s_i 2^(32P) of each coefficient, per-word gathered sums, carries
+// Explicit CRT (crt_coeff) to the symmetric P-word value U_i - s_i 2^(32P)
+// of each coefficient (s_i = top bit of U_i), per-word gathered sums, carries
 // normalised into {-1, 0, 1}.  The ripple is resolved per 32-word step: when
 // no word of the step is 0 or all-ones (a carry can only pass through such a
 // word), word w's incoming carry is just the generated carry g_{w-1}; only
-// otherwise does the warp run the prefix scan of transfer functions.  The
-// post-scale 2^32 N^{-1} mod p comes precomputed from constant memory.
+// otherwise does the warp run the prefix scan of transfer functions.
 // ---------------------------------------------------------------------------
 constexpr int kCrtWarps = 4;       // entries per CTA
 constexpr int kCrtSteps = 8;       // 32-word steps per tile
 constexpr int kCrtTileWords = 32 * kCrtSteps;
 
+// Explicit CRT of one coefficient (constants in CrtConst): the symmetric
+// residue X in (-M_P/4, M_P/4) as P words of two's complement.
 template <int P>
-__device__ __forceinline__ bool garner_coeff(const uint32_t* __restrict__ res, uint64_t res_off,
-                                             int lgN, int64_t ic, uint32_t (&X)[P]) {
+__device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, uint64_t res_off,
+                                          int lgN, int64_t ic, uint32_t (&X)[P]) {
   const uint64_t N = (uint64_t)1 << lgN;
-  uint32_t v[P];
+  uint32_t y[P];
+  uint64_t frac = 0;
 #pragma unroll
-  for (int q = 0; q < P; ++q) {
-    const uint32_t p = c_primes[q].p;
-    uint32_t x = __ldg(res + res_off + (uint64_t)q * N + (uint64_t)ic);
-    x = mul_shoup(x, c_crt.post[lgN][q], c_crt.postq[lgN][q], p);
-    if (q == 0) {
-      v[0] = x;
-    } else {
-      uint32_t t = v[q - 1] >= p ? v[q - 1] - p : v[q - 1];
-#pragma unroll
-      for (int a = q - 2; a >= 0; --a) {
-        const uint32_t va = v[a] >= p ? v[a] - p : v[a];
-        t = add_mod(mul_shoup(t, c_crt.pmod[q][a], c_crt.pmodq[q][a], p), va, p);
-      }
-      v[q] = mul_shoup(sub_mod(x, t, p), c_crt.inv[q], c_crt.invq[q], p);
-    }
+  for (int j = 0; j < P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint32_t x = __ldg(res + res_off + (uint64_t)j * N + (uint64_t)ic);  // [0, 2p)
+    y[j] = redc((uint64_t)x * c_crt.cm[P][lgN][j], p, c_primes[j].pinv);
+    frac += (uint64_t)y[j] * c_crt.fq[j];
   }
+  const uint32_t q = (uint32_t)((frac + (1ull << 57)) >> 58);  // nearest integer
 #pragma unroll
-  for (int q = 0; q < P; ++q) X[q] = 0;
-  X[0] = v[P - 1];
+  for (int w = 0; w < P; ++w) X[w] = 0;
 #pragma unroll
-  for (int i = P - 2; i >= 0; --i) {
-    const uint32_t pi = c_primes[i].p;
-    uint64_t cy = v[i];
+  for (int j = 0; j < P; ++j) {
+    uint64_t cy = 0;
 #pragma unroll
-    for (int q = 0; q < P; ++q) {
-      const uint64_t t = (uint64_t)X[q] * pi + cy;
-      X[q] = (uint32_t)t;
+    for (int w = 0; w < P; ++w) {
+      const uint64_t t = (uint64_t)y[j] * c_crt.mop[P][j][w] + X[w] + cy;
+      X[w] = (uint32_t)t;
       cy = t >> 32;
     }
   }
-  bool gt = false, decided = false;
+  uint32_t br = 0;  // X -= q M_P (mod 2^(32P))
 #pragma unroll
-  for (int q = P - 1; q >= 0; --q) {
-    const uint32_t hq = c_crt.Mhalf[P][q];
-    if (!decided && X[q] != hq) {
-      gt = X[q] > hq;
-      decided = true;
-    }
+  for (int w = 0; w < P; ++w) {
+    const uint64_t t = (uint64_t)q * c_crt.M[P][w] + br;
+    const uint32_t lo = (uint32_t)t;
+    br = (uint32_t)(t >> 32) + (X[w] < lo ? 1u : 0u);
+    X[w] -= lo;
   }
-  if (gt) {
-    uint32_t br = 0;
-#pragma unroll
-    for (int q = 0; q < P; ++q) {
-      const uint64_t t = (uint64_t)X[q] - c_crt.M[P][q] - br;
-      X[q] = (uint32_t)t;
-      br = (uint32_t)(t >> 63);
-    }
-  }
-  return gt;
 }
 
 template <int P>
@@ -538,9 +522,7 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
   const int64_t W = d.out_words;
   const int64_t ncoef = d.ncoef;
   uint32_t* o = out + d.out_word;
-  const int per_warp_words = cmax * P + (cmax + 3) / 4;
-  uint32_t* sU = sm + warp * per_warp_words;
-  uint8_t* sS = reinterpret_cast<uint8_t*>(sU + cmax * P);
+  uint32_t* sU = sm + warp * (cmax * P);  // word q of tile coefficient c at [q * cmax + c]
 
   int hi_prev = 0, carry = 0;
   int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
@@ -553,10 +535,9 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
     const int64_t ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
     for (int64_t c = lane; c < ncf; c += 32) {
       uint32_t X[P];
-      const bool neg = garner_coeff<P>(res, d.res_off, d.lgN, lo_i + c, X);
+      crt_coeff<P>(res, d.res_off, d.lgN, lo_i + c, X);
 #pragma unroll
-      for (int q = 0; q < P; ++q) sU[c * P + q] = X[q];
-      sS[c] = neg ? 1 : 0;
+      for (int q = 0; q < P; ++q) sU[q * cmax + c] = X[q];
     }
     __syncwarp();
     for (int st = 0; st < kCrtSteps; ++st) {
@@ -575,19 +556,21 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
           const int64_t c = i - lo_i;
           const int64_t bi = i * r;
           const int64_t dd = 32 * w - bi;
-          const uint32_t* U = sU + c * P;
+          const uint32_t* U = sU + c;  // word q at U[q * cmax]
           uint32_t slice;
           if (dd < 0) {
             slice = U[0] << (uint32_t)(-dd);
           } else {
             const int64_t q = dd >> 5;
             const uint32_t sh = (uint32_t)(dd & 31);
-            const uint32_t lo = q < P ? U[q] : 0u;
-            const uint32_t hi = q + 1 < P ? U[q + 1] : 0u;
+            const uint32_t lo = q < P ? U[q * cmax] : 0u;
+            const uint32_t hi = q + 1 < P ? U[(q + 1) * cmax] : 0u;
             slice = __funnelshift_r(lo, hi, sh);
           }
           sw += slice;
-          if (sS[c] && (bi >> 5) + P == w) sw -= (int64_t)1 << (bi & 31);
+          // the sign of X_i is the top bit of U_i; its borrow lands in word
+          // (i r) / 32 + P
+          if ((bi >> 5) + P == w && (U[(P - 1) * cmax] >> 31)) sw -= (int64_t)1 << (bi & 31);
         }
       }
       const int hi = active ? (int)(sw >> 32) : 0;
@@ -667,48 +650,78 @@ static int ntt_threads(int lgN) {
 }
 
 template <int D>
-static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx, int count, int P,
-                                 int lgN, const uint64_t* limbs, uint32_t* res, const uint2* twf,
+static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
+                                 const CtaItem* items, int nitems, bool team, int max_lgN,
+                                 const uint64_t* limbs, uint32_t* res, const uint2* twf,
                                  cudaStream_t st) {
-  const int N = 1 << lgN;
-  const bool team = (N >> 3) <= kFwdThreads;
-  const int G = team ? kFwdThreads / (N >> 3) : 1;
-  const size_t smem = sizeof(uint32_t) * (size_t)G * (N + (N >> 5));
-  const int grid = (count + G - 1) / G;
+  const int Nmax = 1 << max_lgN;
+  const size_t smem = team ? sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5))
+                           : sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
   if (team) {
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_fwd2<D, true><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, limbs, res, twf);
+    k_fwd2<D, true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
   } else {
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_fwd2<D, false><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, limbs, res, twf);
+    k_fwd2<D, false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
+  }
+  return cudaGetLastError();
+}
+
+int fwd_team_points() { return 8 * kFwdThreads; }
+
+cudaError_t launch_fwd_items(const FwdDesc* descs, const uint32_t* idx, const CtaItem* items,
+                             int nitems, int D, bool team, int max_lgN, const uint64_t* limbs,
+                             uint32_t* res, const uint2* twf, cudaStream_t st) {
+  if (nitems == 0) return cudaSuccess;
+  switch (D) {
+    case 1: return launch_fwd2_d<1>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 2: return launch_fwd2_d<2>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 3: return launch_fwd2_d<3>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 4: return launch_fwd2_d<4>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 5: return launch_fwd2_d<5>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 6: return launch_fwd2_d<6>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    case 7: return launch_fwd2_d<7>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const CtaItem* items,
+                             int nitems, bool team, int max_lgN, uint32_t* res,
+                             const uint2* twi, cudaStream_t st) {
+  if (nitems == 0) return cudaSuccess;
+  const int Nmax = 1 << max_lgN;
+  const size_t smem = team ? sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5))
+                           : sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
+  if (team) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_inv2<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k_inv2<true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, res, twi);
+  } else {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_inv2<false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k_inv2<false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, res, twi);
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
                              int lgN, const uint64_t* limbs, uint32_t* res,
-                             const uint2* twf, cudaStream_t st, int max_r) {
+                             const uint2* twf, cudaStream_t st) {
   if (count == 0) return cudaSuccess;
-  if (lgN >= 3 && max_r >= 1 && max_r <= 7 * 30) {
-    switch ((max_r + 29) / 30) {
-      case 1: return launch_fwd2_d<1>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 2: return launch_fwd2_d<2>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 3: return launch_fwd2_d<3>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 4: return launch_fwd2_d<4>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 5: return launch_fwd2_d<5>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 6: return launch_fwd2_d<6>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      case 7: return launch_fwd2_d<7>(descs, idx, count, P, lgN, limbs, res, twf, st);
-      default: break;
-    }
-  }
   const size_t smem = sizeof(uint32_t) << lgN;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -723,29 +736,6 @@ cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int coun
 cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count, int P,
                            int lgN, uint32_t* res, const uint2* twi, cudaStream_t st) {
   if (count == 0) return cudaSuccess;
-  if (lgN >= 3) {
-    const int N = 1 << lgN;
-    const bool team = (N >> 3) <= kFwdThreads;
-    const int G = team ? kFwdThreads / (N >> 3) : 1;
-    const size_t smem = sizeof(uint32_t) * (size_t)G * (N + (N >> 5));
-    const int grid = (count + G - 1) / G;
-    if (team) {
-      if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(
-            k_inv2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-      }
-      k_inv2<true><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, res, twi);
-    } else {
-      if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(
-            k_inv2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-      }
-      k_inv2<false><<<grid, kFwdThreads, smem, st>>>(descs, idx, count, lgN, P, res, twi);
-    }
-    return cudaGetLastError();
-  }
   const size_t smem = sizeof(uint32_t) << lgN;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -771,7 +761,7 @@ static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int c
                                 const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
                                 cudaStream_t st) {
   const int cmax = (int)((32 * (int64_t)kCrtTileWords + 32 * P) / rmin + 3);
-  const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P + (cmax + 3) / 4);
+  const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P);
   const size_t smem = per_warp * kCrtWarps;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
   if (smem > 48 * 1024) {

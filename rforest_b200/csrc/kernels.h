@@ -9,16 +9,25 @@ namespace mpzmm {
 
 cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt);
 
-// Split + forward NTT for `count` entries (descriptor indices idx[0..count)),
-// all with transform length 2^lgN and P primes.
-// max_r: the widest coefficient (bits) among the launch's entries.
+// Radix-2 split + forward NTT / inverse NTT, one CTA per (entry, prime),
+// for `count` entries of one class (any lgN >= 1; used for lgN < 3).
 cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
                              int lgN, const uint64_t* limbs, uint32_t* res,
-                             const uint2* twf, cudaStream_t st, int max_r);
-
-// Inverse NTT, in place, for `count` output entries of length 2^lgN.
+                             const uint2* twf, cudaStream_t st);
 cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count, int P,
                            int lgN, uint32_t* res, const uint2* twi, cudaStream_t st);
+
+// Register-blocked transforms (lgN >= 3) over CTA work items of mixed size
+// classes in ONE launch.  team: every item has 2^lgN <= fwd_team_points()
+// (several entries per CTA); otherwise one entry per CTA and max_lgN sizes
+// the shared memory.  D = digits of 30 bits of the widest coefficient.
+int fwd_team_points();
+cudaError_t launch_fwd_items(const FwdDesc* descs, const uint32_t* idx, const CtaItem* items,
+                             int nitems, int D, bool team, int max_lgN, const uint64_t* limbs,
+                             uint32_t* res, const uint2* twf, cudaStream_t st);
+cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const CtaItem* items,
+                             int nitems, bool team, int max_lgN, uint32_t* res,
+                             const uint2* twi, cudaStream_t st);
 
 // CUDA-core contraction over `count` work items.
 cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, int count,

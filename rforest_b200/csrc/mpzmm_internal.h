@@ -34,23 +34,20 @@ struct PrimeConst {
                      // coefficient, with the Montgomery factor folded in
 };
 
-// Garner constants for the first P primes: mixed-radix digits
-//   x = v0 + v1 p0 + v2 p0 p1 + ...
-// v_i = (x_i - (v0 + v1 p0 + ... )) * inv_i mod p_i with inv_i = (p0...p_{i-1})^{-1}.
+// Explicit CRT constants (all exact integers).  For the first P primes with
+// product M_P, a coefficient with residues x_j is
+//     X = sum_j y_j (M_P / p_j) - q M_P,   y_j = x_j (M_P / p_j)^{-1} mod p_j,
+// where q is sum_j y_j / p_j rounded to the nearest integer (computed in
+// 2^-58 fixed point; the planner keeps |X| < M_P / 4, so the rounding has a
+// margin of 1/4 against a fixed-point error below 2^-24).
 struct CrtConst {
-  uint32_t pmod[kMaxPrimes][kMaxPrimes];   // pmod[i][a] = p_a mod p_i  (a < i)
-  uint32_t pmodq[kMaxPrimes][kMaxPrimes];  // Shoup companions
-  uint32_t inv[kMaxPrimes];                // (p0...p_{i-1})^{-1} mod p_i
-  uint32_t invq[kMaxPrimes];
-  // M_P = p0...p_{P-1} and floor(M_P / 2) as little-endian 32-bit words
-  uint32_t M[kMaxPrimes + 1][kMaxCrtWords];
-  uint32_t Mhalf[kMaxPrimes + 1][kMaxCrtWords];
-  int Mwords[kMaxPrimes + 1];              // words of M_P
-  // scale applied to a CRT input residue of a 2^lgN-point transform:
-  // 2^32 N^{-1} mod p_j (removes the contraction's Montgomery factor and the
-  // inverse transform's factor N), with Shoup companions
-  uint32_t post[kMaxLgN + 1][kMaxPrimes];
-  uint32_t postq[kMaxLgN + 1][kMaxPrimes];
+  uint32_t M[kMaxPrimes + 1][kMaxCrtWords];          // M_P, little-endian words
+  int Mwords[kMaxPrimes + 1];
+  uint32_t mop[kMaxPrimes + 1][kMaxPrimes][kMaxPrimes];  // M_P / p_j, P words
+  // Montgomery form (times 2^32) of 2^32 N^{-1} (M_P / p_j)^{-1} mod p_j for
+  // N = 2^lgN: removes the contraction's 2^-32 and the inverse transform's N
+  uint32_t cm[kMaxPrimes + 1][kMaxLgN + 1][kMaxPrimes];
+  uint32_t fq[kMaxPrimes];                           // floor(2^58 / p_j)
 };
 
 // One polynomial (one matrix entry) of the forward transform.
@@ -93,6 +90,16 @@ struct ContractItem {
   uint16_t prime;
   uint16_t pad;
   uint32_t h0;         // first frequency of the block
+};
+
+// Work item of one CTA of the batched transform kernels: `count` entries of
+// one size class (all 2^lgN points, P primes), descriptor indices
+// idx[first .. first + count).
+struct CtaItem {
+  uint32_t first;
+  uint16_t count;
+  uint8_t lgN;
+  uint8_t P;
 };
 
 }  // namespace mpzmm

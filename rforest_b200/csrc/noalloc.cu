@@ -223,9 +223,9 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   const ContractItem* ditems = reinterpret_cast<const ContractItem*>(dd + off_items);
   const uint32_t* didx = reinterpret_cast<const uint32_t*>(dd + off_idx);
 
-  if ((e = launch_split_fwd(dfwd, didx, (int)na, P, lgN, d_a_limbs, dres, ds->twf, s, r)) !=
+  if ((e = launch_split_fwd(dfwd, didx, (int)na, P, lgN, d_a_limbs, dres, ds->twf, s)) !=
           cudaSuccess ||
-      (e = launch_split_fwd(dfwd, didx + na, (int)nb, P, lgN, d_b_limbs, dres, ds->twf, s, r)) !=
+      (e = launch_split_fwd(dfwd, didx + na, (int)nb, P, lgN, d_b_limbs, dres, ds->twf, s)) !=
           cudaSuccess ||
       (e = launch_contract(dpd, ditems, (int)nitems, dres, s)) != cudaSuccess ||
       (e = launch_inv_ntt(dinv, didx + na + nb, (int)nc, P, lgN, dres, ds->twi, s)) !=

@@ -137,42 +137,41 @@ void build(Moduli& M) {
       }
     }
   }
-  // Garner constants
-  for (int i = 1; i < kMaxPrimes; ++i) {
-    const uint32_t p = M.p[i];
-    uint64_t prod = 1;
-    for (int a = 0; a < i; ++a) {
-      const uint32_t pm = M.p[a] % p;
-      M.crt.pmod[i][a] = pm;
-      M.crt.pmodq[i][a] = shoup(pm, p);
-      prod = prod * pm % p;
-    }
-    const uint32_t iv = (uint32_t)powmod(prod, p - 2, p);
-    M.crt.inv[i] = iv;
-    M.crt.invq[i] = shoup(iv, p);
-  }
-  for (int lg = 0; lg <= kMaxLgN; ++lg)
-    for (int j = 0; j < kMaxPrimes; ++j) {
-      const uint32_t p = M.p[j];
-      const uint64_t ninv = powmod((uint64_t)1 << lg, p - 2, p);
-      const uint32_t post = (uint32_t)((((uint64_t)1 << 32) % p) * ninv % p);
-      M.crt.post[lg][j] = post;
-      M.crt.postq[lg][j] = shoup(post, p);
-    }
   std::vector<uint32_t> acc{1};
   for (int P = 1; P <= kMaxPrimes; ++P) {
     mul_small(acc, M.p[P - 1]);
     int words = (int)acc.size();
     M.crt.Mwords[P] = words;
     for (int q = 0; q < words && q < kMaxCrtWords; ++q) M.crt.M[P][q] = acc[q];
-    for (int q = 0; q < words && q < kMaxCrtWords; ++q) {
-      uint32_t hi = (q + 1 < words) ? acc[q + 1] : 0u;
-      M.crt.Mhalf[P][q] = (acc[q] >> 1) | (hi << 31);
-    }
     int top = 31;
     while (!((acc.back() >> top) & 1u)) --top;
     M.mbits[P] = 32 * (words - 1) + top;  // floor(log2 M)
   }
+  // explicit CRT: for P primes, M_P / p_j as P words, and the Montgomery form
+  // of 2^32 N^{-1} (M_P / p_j)^{-1} mod p_j for every transform length
+  for (int P = 1; P <= kMaxPrimes; ++P)
+    for (int j = 0; j < P; ++j) {
+      std::vector<uint32_t> mop{1};
+      uint64_t mop_mod = 1;  // (M_P / p_j) mod p_j
+      const uint32_t pj = M.p[j];
+      for (int a = 0; a < P; ++a) {
+        if (a == j) continue;
+        mul_small(mop, M.p[a]);
+        mop_mod = mop_mod * (M.p[a] % pj) % pj;
+      }
+      for (int w = 0; w < kMaxPrimes; ++w)
+        M.crt.mop[P][j][w] = w < (int)mop.size() ? mop[w] : 0u;
+      const uint64_t inv = powmod(mop_mod, pj - 2, pj);
+      const uint64_t r32 = (((uint64_t)1) << 32) % pj;
+      for (int lg = 0; lg <= kMaxLgN; ++lg) {
+        const uint64_t ninv = powmod((uint64_t)1 << lg, pj - 2, pj);
+        // post = 2^32 N^{-1}; Montgomery form multiplies by 2^32 once more
+        const uint64_t post = r32 * ninv % pj;
+        M.crt.cm[P][lg][j] = (uint32_t)(post * inv % pj * r32 % pj);
+      }
+    }
+  for (int j = 0; j < kMaxPrimes; ++j)
+    M.crt.fq[j] = (uint32_t)((((uint64_t)1) << 58) / M.p[j]);
   M.mbits[0] = 0;
 }
 
@@ -209,7 +208,7 @@ bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* 
   const int64_t ninv = (int64_t)m * n;
   int64_t best = -1;
   for (int P = 2; P <= kMaxPrimes; ++P) {
-    const int budget = M.mbits[P] - 1 - clk;  // 2r + ceil(log2 minlen) <= budget
+    const int budget = M.mbits[P] - 2 - clk;  // 2r + ceil(log2 minlen) <= budget
     if (budget < 3) continue;
     int r = budget / 2;
     if (r > kMaxCoeffBits) r = kMaxCoeffBits;

@@ -35,10 +35,10 @@ int ceil_log2(uint64_t x);
 
 // Picks (P, r, lgN) for an m x k by k x n product whose A / B entries have at
 // most a_bits / b_bits bits.  Every output coefficient c satisfies
-// 2 |c| < p_0...p_{P-1} (proved with the integer bound
-// 1 + ceil(log2 k) + ceil(log2 min(lenA, lenB)) + 2r <= floor(log2 M)), so
-// Garner's symmetric residue recovers it exactly.  Returns false if no
-// supported (P, r, lgN) exists.
+// 4 |c| < p_0...p_{P-1} (proved with the integer bound
+// 2 + ceil(log2 k) + ceil(log2 min(lenA, lenB)) + 2r <= floor(log2 M)), so
+// the symmetric CRT residue is c itself, with the margin the rounded
+// explicit CRT needs.  Returns false if no supported (P, r, lgN) exists.
 bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* out);
 
 // ceil((a_bits + b_bits + ceil(log2 k) + 1) / 64)

@@ -60,15 +60,16 @@ def ntt_primes(count=16):
     (1 << 18, 1 << 10, 16), (1 << 21, 1 << 16, 8), (300, 5, 32), (12345, 678, 3),
     (1 << 21, 1 << 21, 2)])
 def test_params_exactness_bound(product_lib, a_bits, b_bits, k):
-    """Every product coefficient c has 2|c| < p_0...p_{P-1} and the product
-    polynomial fits the transform length."""
+    """Every product coefficient c has 4|c| < p_0...p_{P-1} (the symmetric
+    CRT residue is c, with the margin the rounded explicit CRT needs) and the
+    product polynomial fits the transform length."""
     P, r, lg = api.choose_params(a_bits, b_bits, k)
     primes = ntt_primes()
     M = math.prod(primes[:P])
     lenA = -(-a_bits // r)
     lenB = -(-b_bits // r)
     bound = k * min(lenA, lenB) * ((1 << r) - 1) ** 2
-    assert 2 * bound < M
+    assert 4 * bound < M
     assert lenA + lenB - 1 <= (1 << lg)
     assert 2 <= P <= 16 and lg <= 15
 
