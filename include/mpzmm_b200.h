@@ -96,6 +96,16 @@ MPZMM_API void mpzmm_set_fatal_hook(mpzmm_fatal_fn fn);
 /* Explicit set-up on a device; returns a status.  hw_mpz_setup() calls it
    with the default device. */
 MPZMM_API int mpzmm_setup(int device);
+/* Options (process-wide; a plan keeps the values it was built with).
+   MPZMM_OPT_CONTRACT selects the frequency-domain contraction engine:
+   0 automatic (tensor cores, tcgen05 kind::i8, for products with k >= 24
+   terms and m <= 128, k <= 64, n <= 64; CUDA cores otherwise),
+   1 CUDA cores only, 2 tensor cores wherever the shape allows.
+   The environment variable MPZMM_CONTRACT sets the initial value. */
+#define MPZMM_OPT_CONTRACT 1
+MPZMM_API int mpzmm_set_option(int option, int value);
+MPZMM_API int mpzmm_get_option(int option);
+
 /* Human-readable message for the last error on the calling thread. */
 MPZMM_API const char *mpzmm_last_error(void);
 /* 1 if a CUDA device is usable, else 0 (never aborts). */

@@ -19,6 +19,9 @@ MPZMM_ERR_STATE = 6
 MPZMM_ERR_TIMEOUT = 7
 MPZMM_ERR_BUSY = 8
 
+MPZMM_OPT_CONTRACT = 1
+CONTRACT_AUTO, CONTRACT_CUDA_CORES, CONTRACT_TENSOR_CORES = 0, 1, 2
+
 u64p = C.POINTER(C.c_uint64)
 i64p = C.POINTER(C.c_int64)
 i32p = C.POINTER(C.c_int32)
@@ -66,6 +69,8 @@ def lib():
         "mpz_rmatrix_gpu_fft_suitable": (C.c_int, [vp, C.c_int, vp, C.c_int]),
         "mpzmm_set_fatal_hook": (None, [vp]),
         "mpzmm_setup": (C.c_int, [C.c_int]),
+        "mpzmm_set_option": (C.c_int, [C.c_int, C.c_int]),
+        "mpzmm_get_option": (C.c_int, [C.c_int]),
         "mpzmm_last_error": (C.c_char_p, []),
         "mpzmm_device_available": (C.c_int, []),
         "mpzmm_matmul": (C.c_int, [C.c_int, C.c_int, C.c_int, u64p, i64p, i32p, u64p, i64p,

@@ -35,6 +35,15 @@ def setup(device: int = 0) -> None:
     _lib.check(_lib.lib().mpzmm_setup(device))
 
 
+def set_contract_mode(mode: int) -> None:
+    """0 automatic, 1 CUDA cores only, 2 tensor cores wherever the shape allows."""
+    _lib.check(_lib.lib().mpzmm_set_option(_lib.MPZMM_OPT_CONTRACT, mode))
+
+
+def contract_mode() -> int:
+    return int(_lib.lib().mpzmm_get_option(_lib.MPZMM_OPT_CONTRACT))
+
+
 def device_available() -> bool:
     return bool(_lib.lib().mpzmm_device_available())
 

@@ -92,6 +92,20 @@ void mpzmm_set_fatal_hook(mpzmm_fatal_fn fn) { g_fatal = fn ? fn : default_fatal
 
 int mpzmm_setup(int device) { return ensure_setup(device); }
 
+int mpzmm_set_option(int option, int value) {
+  if (option == MPZMM_OPT_CONTRACT) {
+    if (value < 0 || value > 2) return set_error(kErrArg, "contract mode must be 0, 1 or 2");
+    context().contract_mode = value;
+    return kOk;
+  }
+  return set_error(kErrArg, "unknown option");
+}
+
+int mpzmm_get_option(int option) {
+  if (option == MPZMM_OPT_CONTRACT) return context().contract_mode;
+  return -1;
+}
+
 const char* mpzmm_last_error(void) { return last_error(); }
 
 int mpzmm_device_available(void) {

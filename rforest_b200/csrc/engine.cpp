@@ -124,6 +124,10 @@ int ensure_setup(int device) {
      "copy twiddles");
   CU(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking), "cudaStreamCreate");
   g_ctx.ws = new Workspace;
+  if (const char* cm = std::getenv("MPZMM_CONTRACT")) {
+    const int v = std::atoi(cm);
+    if (v >= 0 && v <= 2) g_ctx.contract_mode = v;
+  }
   g_ctx.device = device;
   g_ctx.ready = true;
   return kOk;
@@ -204,6 +208,14 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   if ((st = grow_dev(&d_out, cap_out, out_words, 4))) return st;
   if ((st = grow_dev(&d_sizes, cap_sizes, sizes, 4))) return st;
   if ((st = grow_dev(&d_desc, cap_desc, desc_bytes, 1))) return st;
+  if (!d_status) {
+    cudaError_t e = cudaMalloc((void**)&d_status, sizeof(int));
+    if (e != cudaSuccess) {
+      d_status = nullptr;
+      return set_error(kErrNoMem, std::string("cudaMalloc(status): ") + cudaGetErrorString(e));
+    }
+    device_bytes += (int64_t)sizeof(int);
+  }
   if ((st = grow_host(&h_limbs, hcap_limbs, limbs, 8))) return st;
   if ((st = grow_host(&h_out, hcap_out, out_words, 4))) return st;
   if ((st = grow_host(&h_sizes, hcap_sizes, sizes, 4))) return st;
@@ -217,6 +229,8 @@ void Workspace::release() {
   cudaFree(d_out);
   cudaFree(d_sizes);
   cudaFree(d_desc);
+  cudaFree(d_status);
+  d_status = nullptr;
   cudaFreeHost(h_limbs);
   cudaFreeHost(h_out);
   cudaFreeHost(h_sizes);
@@ -320,14 +334,22 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     }
     const uint32_t prod_index = (uint32_t)pd_.size();
     pd_.push_back(pd);
+    const int mode = context().contract_mode;
+    const bool use_tc = contract_tc_eligible(m, k, n) &&
+                        (mode == 2 || (mode == 0 && k >= kTcMinK));
+    if (use_tc) {
+      if (k > tc_max_k_) tc_max_k_ = k;
+      if (n > tc_max_n_) tc_max_n_ = n;
+    }
+    const uint64_t fstep = use_tc ? (uint64_t)kTcFreqsPerCta : (uint64_t)block_freqs;
     for (int j = 0; j < P; ++j)
-      for (uint64_t h0 = 0; h0 < N; h0 += (uint64_t)block_freqs) {
+      for (uint64_t h0 = 0; h0 < N; h0 += fstep) {
         ContractItem it;
         it.prod = prod_index;
         it.prime = (uint16_t)j;
         it.pad = 0;
         it.h0 = (uint32_t)h0;
-        items_.push_back(it);
+        (use_tc ? tc_items_ : items_).push_back(it);
       }
     const uint64_t ncoef_c = (uint64_t)(prm.lenA + prm.lenB - 1);
     for (int e = 0; e < m * n; ++e) {
@@ -425,7 +447,8 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   off_inv_ = align16(off_fwd_ + fwd_.size() * sizeof(FwdDesc));
   off_pd_ = align16(off_inv_ + inv_.size() * sizeof(InvDesc));
   off_items_ = align16(off_pd_ + pd_.size() * sizeof(ProdDesc));
-  off_idx_ = align16(off_items_ + items_.size() * sizeof(ContractItem));
+  off_tc_ = align16(off_items_ + items_.size() * sizeof(ContractItem));
+  off_idx_ = align16(off_tc_ + tc_items_.size() * sizeof(ContractItem));
   off_cta_ = align16(off_idx_ + idx_all_.size() * sizeof(uint32_t));
   desc_bytes_ = align16(off_cta_ + cta_items_.size() * sizeof(CtaItem));
   ws_ = ws ? ws : &own_;
@@ -437,6 +460,8 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   if (!pd_.empty()) std::memcpy(hd + off_pd_, pd_.data(), pd_.size() * sizeof(ProdDesc));
   if (!items_.empty())
     std::memcpy(hd + off_items_, items_.data(), items_.size() * sizeof(ContractItem));
+  if (!tc_items_.empty())
+    std::memcpy(hd + off_tc_, tc_items_.data(), tc_items_.size() * sizeof(ContractItem));
   if (!idx_all_.empty())
     std::memcpy(hd + off_idx_, idx_all_.data(), idx_all_.size() * sizeof(uint32_t));
   if (!cta_items_.empty())
@@ -445,9 +470,11 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   d_inv_ = reinterpret_cast<InvDesc*>(ws_->d_desc + off_inv_);
   d_pd_ = reinterpret_cast<ProdDesc*>(ws_->d_desc + off_pd_);
   d_items_ = reinterpret_cast<ContractItem*>(ws_->d_desc + off_items_);
+  d_tc_items_ = reinterpret_cast<ContractItem*>(ws_->d_desc + off_tc_);
   d_idx_ = reinterpret_cast<uint32_t*>(ws_->d_desc + off_idx_);
   d_cta_ = reinterpret_cast<CtaItem*>(ws_->d_desc + off_cta_);
   launches_ = (int64_t)fwd_groups_.size() + (items_.empty() ? 0 : 1) +
+              (tc_items_.empty() ? 0 : 1) +
               (int64_t)inv_groups_.size() + (int64_t)rec_groups_.size();
   built_ = true;
   return kOk;
@@ -486,6 +513,7 @@ int Plan::upload(cudaStream_t st) {
   if (desc_bytes_)
     CU(cudaMemcpyAsync(ws_->d_desc, ws_->h_desc, desc_bytes_, cudaMemcpyHostToDevice, st),
        "H2D descriptors");
+  CU(cudaMemsetAsync(ws_->d_status, 0, sizeof(int), st), "clear status");
   if (n_limbs_)
     CU(cudaMemcpyAsync(ws_->d_limbs, hl, n_limbs_ * 8, cudaMemcpyHostToDevice, st), "H2D limbs");
   return kOk;
@@ -515,6 +543,10 @@ int Plan::execute(cudaStream_t st) {
   if (timing_) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
+  if (!tc_items_.empty())
+    CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, kTcFreqsPerCta,
+                          tc_max_k_, tc_max_n_, ws_->d_status, st),
+       "tensor-core contraction launch");
   if (timing_) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
   for (const Group& g : inv_groups_) {
     if (g.batched)
@@ -556,7 +588,7 @@ int Plan::stage_times(float ms[kStages], int64_t* executes) {
 
 void Plan::stage_launches(int64_t out[kStages]) const {
   out[0] = (int64_t)fwd_groups_.size();
-  out[1] = items_.empty() ? 0 : 1;
+  out[1] = (items_.empty() ? 0 : 1) + (tc_items_.empty() ? 0 : 1);
   out[2] = (int64_t)inv_groups_.size();
   out[3] = (int64_t)rec_groups_.size();
 }
@@ -571,7 +603,12 @@ int Plan::download(cudaStream_t st) {
        "D2H sizes");
   if (n_out_words_)
     CU(cudaMemcpyAsync(ho, ws_->d_out, n_out_words_ * 4, cudaMemcpyDeviceToHost, st), "D2H words");
+  int kstatus = 0;
+  CU(cudaMemcpyAsync(&kstatus, ws_->d_status, sizeof(int), cudaMemcpyDeviceToHost, st),
+     "D2H status");
   CU(cudaStreamSynchronize(st), "kernel execution");
+  if (kstatus)
+    return set_error(kErrTimeout, "a tensor-core contraction wait timed out; results invalid");
   // capacity check first (serial, cheap), then the copies in parallel
   int status = kOk;
   std::vector<uint8_t> ok(outs_.size(), 1);

@@ -61,6 +61,7 @@ struct Workspace {
   uint32_t* d_out = nullptr;
   int32_t* d_sizes = nullptr;
   uint8_t* d_desc = nullptr;
+  int* d_status = nullptr;  // nonzero: a kernel's bounded wait gave up
   uint64_t* h_limbs = nullptr;
   uint32_t* h_out = nullptr;
   int32_t* h_sizes = nullptr;
@@ -83,7 +84,15 @@ struct Context {
   uint2* d_twi = nullptr;
   int num_sms = 0;
   Workspace* ws = nullptr;  // shared by one-shot calls (guarded by ws_mu)
+  // contraction engine: 0 automatic (tensor cores from kTcMinK terms on),
+  // 1 CUDA cores only, 2 tensor cores wherever the shape allows
+  int contract_mode = 0;
 };
+
+// Products with at least this many terms use the tensor-core contraction in
+// automatic mode (below it the byte split costs more than it saves).
+constexpr int kTcMinK = 24;
+constexpr int kTcFreqsPerCta = 16;
 
 Context& context();
 std::mutex& workspace_mutex();
@@ -139,7 +148,9 @@ class Plan {
   std::vector<FwdDesc> fwd_;
   std::vector<InvDesc> inv_;
   std::vector<ProdDesc> pd_;
-  std::vector<ContractItem> items_;
+  std::vector<ContractItem> items_;     // CUDA-core contraction work
+  std::vector<ContractItem> tc_items_;  // tensor-core contraction work
+  int tc_max_k_ = 0, tc_max_n_ = 0;
   std::vector<Group> fwd_groups_, inv_groups_, rec_groups_;
   std::vector<uint32_t> idx_all_;
   std::vector<CtaItem> cta_items_;
@@ -160,6 +171,8 @@ class Plan {
   InvDesc* d_inv_ = nullptr;
   ProdDesc* d_pd_ = nullptr;
   ContractItem* d_items_ = nullptr;
+  ContractItem* d_tc_items_ = nullptr;
+  size_t off_tc_ = 0;
   uint32_t* d_idx_ = nullptr;
   bool built_ = false;
   bool timing_ = false;

@@ -23,6 +23,7 @@
 #include "modarith.cuh"
 #include "mpzmm_internal.h"
 #include "ntt_fast.cuh"
+#include "contract_tc.cuh"
 
 namespace mpzmm {
 
@@ -635,6 +636,145 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Tensor-core contraction (see contract_tc.cuh for the exact-split scheme).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(tc::kThreads, 1)
+k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
+              uint32_t* __restrict__ res, int fb, int* __restrict__ status) {
+  extern __shared__ __align__(1024) uint8_t tsm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  const ContractItem it = items[blockIdx.x];
+  const ProdDesc d = prods[it.prod];
+  const int m = d.m, k = d.k, n = d.n;
+  const int N = 1 << d.lgN;
+  const int j = it.prime;
+  const uint32_t p = c_primes[j].p;
+  const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
+  const uint32_t kprime = (uint32_t)((4 * k + 31) & ~31);
+  const uint32_t ncols = (uint32_t)((8 * n + 15) & ~15);  // B' rows = D columns
+  uint8_t* As = tsm;
+  uint8_t* Bs = tsm + 128u * kprime;
+  const uint32_t tile_bytes = (128u + ncols) * kprime;
+
+  // zero both tiles once: padding rows/columns stay zero for every frequency
+  for (uint32_t o = 16u * tid; o < tile_bytes; o += 16u * tc::kThreads)
+    *reinterpret_cast<uint4*>(tsm + o) = make_uint4(0, 0, 0, 0);
+  if (warp == 0) {
+    const uint32_t slot = tc::smem_u32(&tmem_slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(slot), "r"((uint32_t)tc::kTmemCols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(tc::smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t barp = tc::smem_u32(&bar);
+  uint32_t phase = 0;
+  const uint64_t bias = c_primes[j].bias;
+  const uint32_t pinv = c_primes[j].pinv;
+  const uint32_t mu = c_primes[j].mu;
+
+  for (int f = 0; f < fb; ++f) {
+    const uint32_t h = it.h0 + (uint32_t)f;
+    if (h >= (uint32_t)N) break;  // uniform over the CTA
+    const uint64_t base = (uint64_t)j * (uint64_t)N + h;
+    // stage A' (row i, bytes 4kk..4kk+3) and B' (rows 8l+u, same bytes)
+    for (int idx = tid; idx < m * k; idx += tc::kThreads) {
+      const int i = idx / k, kk = idx - (idx / k) * k;
+      const uint32_t x = __ldg(res + d.a_res + (uint64_t)(i * k + kk) * stride + base);
+      *reinterpret_cast<uint32_t*>(As + tc::tile_off((uint32_t)i, 4u * kk, kprime)) =
+          tc::split_bytes(x, p);
+    }
+    for (int idx = tid; idx < k * n; idx += tc::kThreads) {
+      const int kk = idx / n, l = idx - (idx / n) * n;
+      const uint32_t x = __ldg(res + d.b_res + (uint64_t)(kk * n + l) * stride + base);
+      const uint32_t rev = __byte_perm(tc::split_bytes(x, p), 0u, 0x0123u);  // d3 d2 d1 d0
+      const uint64_t T = (uint64_t)rev << 32;
+#pragma unroll
+      for (int u = 0; u < 7; ++u)
+        *reinterpret_cast<uint32_t*>(Bs + tc::tile_off((uint32_t)(8 * l + u), 4u * kk, kprime)) =
+            (uint32_t)(T >> (8 * (7 - u)));
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (uint32_t t0 = 0; t0 < ncols; t0 += 256) {
+        const uint32_t nt = (ncols - t0) < 256u ? (ncols - t0) : 256u;
+        const uint32_t idesc = tc::idesc_i8(nt);
+        for (uint32_t ks = 0; ks < kprime / 32; ++ks) {
+          const uint64_t ad = tc::smem_desc(tc::smem_u32(As) + 256u * ks, kprime);
+          const uint64_t bd = tc::smem_desc(tc::smem_u32(Bs) + t0 * kprime + 256u * ks, kprime);
+          const uint32_t acc = ks > 0 ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+              :: "r"(tmem + t0), "l"(ad), "l"(bd), "r"(idesc), "r"(acc),
+                 "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(barp) : "memory");
+    }
+    const bool ok = tc::mbar_wait(barp, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {  // every thread takes the same branch
+      if (tid == 0) atomicExch(status, 1);
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i
+    const int i = 32 * warp + lane;
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    for (int l0 = 0; l0 < n; l0 += 4) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+            "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+            "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+            "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(lane_addr + 8u * (uint32_t)l0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (i < m) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int l = l0 + q;
+          if (l < n) {
+            int64_t z = 0;
+#pragma unroll
+            for (int u = 0; u < 7; ++u) z += (int64_t)(int32_t)v[8 * q + u] * c_primes[j].w8[u];
+            const uint32_t out = redc64((uint64_t)(z + (int64_t)bias), p, pinv, mu);
+            res[d.c_res + (uint64_t)(i * n + l) * stride + base] = out;
+          }
+        }
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(tmem), "r"((uint32_t)tc::kTmemCols) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -755,6 +895,26 @@ cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, in
 }
 
 int contract_block_freqs() { return kContractThreads; }
+
+bool contract_tc_eligible(int m, int k, int n) {
+  return m >= 1 && m <= tc::kMaxM && k >= 1 && k <= tc::kMaxK && n >= 1 && n <= tc::kMaxN;
+}
+
+cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
+                               uint32_t* res, int fb, int max_k, int max_n, int* status,
+                               cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  const size_t kprime = (size_t)((4 * max_k + 31) & ~31);
+  const size_t ncols = (size_t)((8 * max_n + 15) & ~15);
+  size_t smem = (128 + ncols) * kprime;
+  // at least 120 KB so that one CTA (512 TMEM columns) runs per SM
+  if (smem < 120 * 1024) smem = 120 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  k_contract_tc<<<count, tc::kThreads, smem, st>>>(prods, items, res, fb, status);
+  return cudaGetLastError();
+}
 
 template <int P>
 static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int count,

@@ -34,6 +34,14 @@ cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, in
                             uint32_t* res, cudaStream_t st);
 int contract_block_freqs();
 
+// Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
+// k <= 64, n <= 64; each work item covers `fb` consecutive frequencies.
+// *status is set to 1 if a bounded wait gave up.
+bool contract_tc_eligible(int m, int k, int n);
+cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
+                               uint32_t* res, int fb, int max_k, int max_n, int* status,
+                               cudaStream_t st);
+
 // CRT + recompose + sign for `count` output entries with P primes; rmin is
 // the narrowest coefficient width among them (it sizes the shared scratch).
 cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int count, int P,

@@ -32,6 +32,8 @@ struct PrimeConst {
   uint32_t pad;
   uint32_t dig[8];   // 2^(30 q + 32) mod p: weights of the 30-bit digits of a
                      // coefficient, with the Montgomery factor folded in
+  uint32_t w8[8];    // 2^(8 u) mod p: weights of the byte convolutions (tensor cores)
+  uint64_t bias;     // a multiple of p >= 2^56 (makes signed sums non-negative)
 };
 
 // Explicit CRT constants (all exact integers).  For the first P primes with

@@ -121,6 +121,8 @@ void build(Moduli& M) {
     pc.b32 = (uint32_t)((((uint64_t)1) << 32) % p);
     pc.b32q = shoup(pc.b32, p);
     for (int q = 0; q < 8; ++q) pc.dig[q] = (uint32_t)powmod(2, (uint64_t)(30 * q + 32), p);
+    for (int u = 0; u < 8; ++u) pc.w8[u] = (uint32_t)powmod(2, (uint64_t)(8 * u), p);
+    pc.bias = ((((uint64_t)1 << 56) + p - 1) / p) * p;
     const uint32_t g = primitive_root(p);
     const uint64_t wmax = powmod(g, (p - 1) >> kTwiddleLg, p);  // order 2^kTwiddleLg
     for (int lgm = 0; lgm < kTwiddleLg; ++lgm) {

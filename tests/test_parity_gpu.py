@@ -153,3 +153,67 @@ def test_config4_full_size(gpu):
         for j in range(0, 64, 5):
             s = sum(Aq[i * 64 + l] * Bq[l * 64 + j] for l in range(64)) % q
             assert s == Cq[i * 64 + j]
+
+
+# ---------------------------------------------------------------------------
+# the tensor-core contraction (tcgen05 kind::i8), forced on every eligible
+# product, against the same goldens / Python integers
+# ---------------------------------------------------------------------------
+@pytest.fixture
+def tensor_cores(gpu):
+    api.set_contract_mode(2)
+    yield
+    api.set_contract_mode(0)
+
+
+@pytest.fixture
+def cuda_cores(gpu):
+    api.set_contract_mode(1)
+    yield
+    api.set_contract_mode(0)
+
+
+def test_tc_config1_and_edges(tensor_cores):
+    A, B, Cexp = G.config1()
+    assert api.matmul(4, 4, 4, A, B).to_ints() == Cexp.to_ints()
+    for (m, k, n, A, B, Cexp) in G.edge_cases():
+        assert api.matmul(m, k, n, A, B).to_ints() == Cexp.to_ints(), (m, k, n)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_tc_random_shapes(tensor_cores, seed):
+    rng = random.Random(500 + seed)
+    for _ in range(6):
+        m, k, n = rng.randint(1, 40), rng.choice([1, 2, 7, 8, 31, 32, 33, 64]), rng.randint(1, 64)
+        bits = rng.choice([64, 300, 2000, 9000])
+        Ai = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(m * k)]
+        Bi = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(k * n)]
+        C = api.matmul(m, k, n, PK.from_ints(Ai), PK.from_ints(Bi))
+        want = [sum(Ai[i * k + l] * Bi[l * n + j] for l in range(k))
+                for i in range(m) for j in range(n)]
+        assert C.to_ints() == want, (m, k, n, bits)
+
+
+def test_tc_config2_golden(tensor_cores):
+    p = W.config2()
+    assert PK.digest(api.matmul(8, 8, 8, p.A, p.B)) == G.digests()["config2"]["C"]
+
+
+def test_tc_batch_matches_cuda_cores(gpu):
+    prods = [W.random_product(9, t, 2, 40, 8, 14) for t in range(12)]
+    trip = [(p.m, p.k, p.n, p.A, p.B) for p in prods]
+    api.set_contract_mode(1)
+    try:
+        a = [PK.digest(c) for c in api.matmul_batch(trip)]
+        api.set_contract_mode(2)
+        b = [PK.digest(c) for c in api.matmul_batch(trip)]
+    finally:
+        api.set_contract_mode(0)
+    assert a == b
+
+
+def test_tc_config4_full_size(tensor_cores):
+    p = W.config4()
+    C = api.matmul(64, 64, 64, p.A, p.B)
+    d = G.digests()
+    assert PK.digest(C) == d["config4"]["C"]
