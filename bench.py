@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["config3", "config2", "config4", "config1"],
+    ap.add_argument("--workload", choices=["config3", "config2", "config4", "config1",
+                                           "config4_small"],
                     default="config3")
     ap.add_argument("--count", type=int, default=4096, help="products per batch (config3)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -51,6 +52,12 @@ def parse():
                     help="products in the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--contract", choices=["auto", "cuda", "tc"], default="auto",
+                    help="contraction engine of the headline measurement")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the plain one-product-per-call and forced tensor-core lines")
+    ap.add_argument("--plain-sample", type=int, default=256,
+                    help="products timed one call each for the plain comparison")
     return ap.parse_args()
 
 
@@ -65,6 +72,8 @@ def make_workload(name, replicate, count):
         return [W.config2(replicate)]
     if name == "config4":
         return [W.config4(replicate)]
+    if name == "config4_small":
+        return [W.config4(replicate, bits=1 << 16)]
     return [W.config1(replicate)]
 
 
@@ -79,6 +88,9 @@ def workload_config(name, count):
     if name == "config4":
         return {"workload": "single 64x64x64 exact matmul", "products_per_step": 1,
                 "bits": "2^20, unsigned", "seed": 4001}
+    if name == "config4_small":
+        return {"workload": "single 64x64x64 exact matmul (profiling size)",
+                "products_per_step": 1, "bits": "2^16, unsigned", "seed": 4001}
     return {"workload": "single 4x4x4 exact matmul", "products_per_step": 1,
             "bits": "4096, signed", "seed": 1001}
 
@@ -294,6 +306,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     api.setup(local_rank)
+    modes = {"auto": 0, "cuda": 1, "tc": 2}
+    api.set_contract_mode(modes[args.contract])
     stream = torch.cuda.Stream()
 
     replicate = 1 + rank
@@ -365,6 +379,11 @@ def main():
         d2h_words += p.m * p.n * cap
     d2h = d2h_words * 8
 
+    comparisons = None
+    if not args.no_compare and args.workload == "config3":
+        comparisons = compare_forms(api, torch, stream, triples, args)
+        api.set_contract_mode(modes[args.contract])
+
     if rank == 0:
         # roofline of the dominant stage (3-pass model, reference parameters)
         b1, b2, b3 = pass_bytes(prods, out_limbs)
@@ -408,11 +427,60 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "verified": verified,
+            "comparisons": comparisons,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def device_time_ms(torch, stream, fn, reps):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def compare_forms(api, torch, stream, triples, args):
+    """Batched forms against the plain one-product-per-call CUDA-core form."""
+    out = {}
+    # batched, tensor-core contraction forced on every eligible product
+    api.set_contract_mode(2)
+    plan = api.Plan(triples, stream=stream)
+    for _ in range(2):
+        plan.execute(stream)
+    ms = device_time_ms(torch, stream, lambda: plan.execute(stream), max(2, args.steps // 2))
+    out["batched_tensor_cores"] = {"value": len(triples) * max(2, args.steps // 2) / (ms / 1e3),
+                                   "unit": UNIT, "timing": "device, inputs resident"}
+    plan.close()
+    # plain: one product per call, CUDA-core contraction
+    api.set_contract_mode(1)
+    sample = triples[:args.plain_sample]
+    plans = [api.Plan([t], stream=stream) for t in sample]
+    for pl in plans:
+        pl.execute(stream)
+    ms = device_time_ms(torch, stream, lambda: [pl.execute(stream) for pl in plans], 1)
+    out["plain_one_per_call_resident"] = {
+        "value": len(sample) / (ms / 1e3), "unit": UNIT,
+        "timing": f"device, one plan execute per product, first {len(sample)} products"}
+    for pl in plans:
+        pl.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for t in sample:
+        api.matmul(*t, stream=stream)
+    dt = time.perf_counter() - t0
+    out["plain_one_per_call_e2e"] = {
+        "value": len(sample) / dt, "unit": UNIT,
+        "timing": f"wall clock, mpzmm_matmul per product with host buffers, first {len(sample)}"}
+    api.set_contract_mode(0)
+    return out
 
 
 def load_peaks():
