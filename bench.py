@@ -58,6 +58,11 @@ def parse():
                     help="skip the plain one-product-per-call and forced tensor-core lines")
     ap.add_argument("--plain-sample", type=int, default=256,
                     help="products timed one call each for the plain comparison")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--serve-pool", type=int, default=96,
+                    help="distinct serving requests (config-5 draws), cycled")
+    ap.add_argument("--serve-requests", type=int, default=400,
+                    help="requests per open-loop serving run")
     return ap.parse_args()
 
 
@@ -309,6 +314,7 @@ def main():
     modes = {"auto": 0, "cuda": 1, "tc": 2}
     api.set_contract_mode(modes[args.contract])
     stream = torch.cuda.Stream()
+    tuning = api.autotune(stream)
 
     replicate = 1 + rank
     prods = make_workload(args.workload, replicate, args.count)
@@ -345,6 +351,12 @@ def main():
         dist.barrier()
     value = units_per_rank * world * args.steps / (ms / 1000.0)
 
+    # the same plan replayed as one CUDA graph per step
+    plan.set_graph(True)
+    plan.execute(stream)
+    ms_graph = device_time_ms(torch, stream, lambda: plan.execute(stream), args.steps)
+    value_graph = units_per_rank * args.steps / (ms_graph / 1000.0)
+
     outs = plan.download(stream)
     out_limbs = [int(np.abs(c.sizes.astype(np.int64)).sum()) for c in outs]
     verified = None
@@ -378,6 +390,10 @@ def main():
         cap = api.output_limbs(p.k, 64 * p.A.max_limbs(), 64 * p.B.max_limbs())
         d2h_words += p.m * p.n * cap
     d2h = d2h_words * 8
+
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving and args.workload == "config3":
+        serving = serving_benchmark(api, args)
 
     comparisons = None
     if not args.no_compare and args.workload == "config3":
@@ -414,10 +430,13 @@ def main():
             "config": dict(workload_config(args.workload, args.count),
                            l2="inputs larger than L2 (residues of the batch >> 126 MB)",
                            params_product0=info, device_bytes=info["device_bytes"],
-                           e2e_steps=e2e_steps, parallelism=f"replicas x{world}"),
+                           e2e_steps=e2e_steps, parallelism=f"replicas x{world}",
+                           contract=args.contract,
+                           autotune_contract_ms={str(k): v for k, v in tuning.items()}),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(stage_launches) * args.steps),
+            "value_cuda_graph": value_graph,
             "stages_ms_per_step": {n: round(t / max(1, timed), 4)
                                    for n, t in zip(names, stage_ms)},
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved,
@@ -428,6 +447,7 @@ def main():
             "clocks": clk,
             "verified": verified,
             "comparisons": comparisons,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -480,6 +500,91 @@ def compare_forms(api, torch, stream, triples, args):
         "value": len(sample) / dt, "unit": UNIT,
         "timing": f"wall clock, mpzmm_matmul per product with host buffers, first {len(sample)}"}
     api.set_contract_mode(0)
+    return out
+
+
+def _pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    i = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[i]
+
+
+def serving_benchmark(api, args):
+    """Open-loop serving of config-5 requests (m,k,n uniform in 2..32, entry
+    bit lengths log-uniform in [2^8, 2^20], signed) through the continuous-
+    batching server: saturation throughput, then Poisson arrivals at 0.5, 0.8
+    and 0.95 of it with p50/p99 latency (submit to result in host memory).
+    A pool of distinct seeded requests is cycled to bound host memory."""
+    import threading
+    from rforest_b200 import workloads as W
+    pool = [W.config5_request(1, t) for t in range(args.serve_pool)]
+    trip = [(p.m, p.k, p.n, p.A, p.B) for p in pool]
+    out = {"workload": "config-5 requests: m,k,n uniform in {2..32}, bits log-uniform "
+                       "[2^8, 2^20], signed", "pool": len(pool)}
+    # plain GPU path: one call per request over the whole pool, no batching
+    for t in trip[:4]:
+        api.matmul(*t)
+    t0 = time.perf_counter()
+    for t in trip:
+        api.matmul(*t)
+    out["plain_one_call_per_request"] = {"value": len(trip) / (time.perf_counter() - t0),
+                                         "unit": "requests/s",
+                                         "note": "mpzmm_matmul per request, same pool"}
+    srv = api.Server(slots=3, max_batch=32)
+    out["server_config"] = {"slots": 3, "max_batch": 32, "budget": "3/4 of free memory"}
+    try:
+        # warm-up: two passes of the pool grow every slot's pinned staging and
+        # the device memory pool, so the timed runs measure steady state
+        tickets = [srv.submit(*trip[i % len(trip)]) for i in range(2 * len(trip))]
+        for t in tickets:
+            srv.wait(t, 600000)
+            srv.release(t)
+        # saturation: everything queued at once
+        nsat = max(len(trip), 2 * len(trip))
+        t0 = time.perf_counter()
+        tickets = [srv.submit(*trip[i % len(trip)]) for i in range(nsat)]
+        for t in tickets:
+            srv.wait(t, 600000)
+        sat = nsat / (time.perf_counter() - t0)
+        for t in tickets:
+            srv.release(t)
+        out["saturation"] = {"value": sat, "unit": "requests/s"}
+        runs = []
+        for frac in (0.5, 0.8, 0.95):
+            lam = frac * sat
+            R = int(max(64, min(args.serve_requests, lam * 6.0)))
+            arr = W.poisson_arrivals(1, R, lam)
+            tickets = [None] * R
+
+            def feeder():
+                base = time.perf_counter()
+                for i in range(R):
+                    delay = base + float(arr[i]) - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    tickets[i] = srv.submit(*trip[i % len(trip)])
+
+            th = threading.Thread(target=feeder)
+            th.start()
+            th.join()
+            lat, subs, dones = [], [], []
+            for t in tickets:
+                srv.wait(t, 600000)
+                s0, _, d0 = srv.times(t)
+                lat.append((d0 - s0) / 1e6)
+                subs.append(s0)
+                dones.append(d0)
+                srv.release(t)
+            span = (max(dones) - min(subs)) / 1e9
+            runs.append({"load": frac, "offered": lam, "requests": R,
+                         "throughput": R / span, "p50_ms": _pct(lat, 50),
+                         "p99_ms": _pct(lat, 99), "unit": "requests/s"})
+        out["runs"] = runs
+        out["server"] = srv.stats()
+    finally:
+        srv.close()
     return out
 
 

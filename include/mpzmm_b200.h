@@ -98,13 +98,20 @@ MPZMM_API void mpzmm_set_fatal_hook(mpzmm_fatal_fn fn);
 MPZMM_API int mpzmm_setup(int device);
 /* Options (process-wide; a plan keeps the values it was built with).
    MPZMM_OPT_CONTRACT selects the frequency-domain contraction engine:
-   0 automatic (tensor cores, tcgen05 kind::i8, for products with k >= 24
-   terms and m <= 128, k <= 64, n <= 64; CUDA cores otherwise),
+   0 automatic (per size class, the engine mpzmm_autotune measured faster;
+   tensor cores -- tcgen05 kind::i8 -- only for m <= 128, k <= 64, n <= 64),
    1 CUDA cores only, 2 tensor cores wherever the shape allows.
    The environment variable MPZMM_CONTRACT sets the initial value. */
 #define MPZMM_OPT_CONTRACT 1
 MPZMM_API int mpzmm_set_option(int option, int value);
 MPZMM_API int mpzmm_get_option(int option);
+
+/* Autotuner: times the contraction of a representative product per size
+   class (32 x k by k x 32 with k = 8, 16, 32, 64, 2^14-bit entries) on CUDA
+   cores and on tensor cores and makes automatic mode use the faster engine
+   for that class (until then automatic mode uses CUDA cores).  ms_out, if
+   not NULL, receives 8 floats: {CUDA, tensor} milliseconds per class. */
+MPZMM_API int mpzmm_autotune(void *stream, float *ms_out);
 
 /* Human-readable message for the last error on the calling thread. */
 MPZMM_API const char *mpzmm_last_error(void);
@@ -164,6 +171,11 @@ MPZMM_API int mpzmm_plan_download(mpzmm_plan *plan, void *stream);
 MPZMM_API int mpzmm_plan_upload(mpzmm_plan *plan, void *stream);
 MPZMM_API void mpzmm_plan_destroy(mpzmm_plan *plan);
 
+/* CUDA-graph mode (off by default): the first execute captures every launch
+   of the plan into a CUDA graph on its stream; later executes replay it as one
+   graph launch.  Ignored while stage timing is on. */
+MPZMM_API int mpzmm_plan_set_graph(mpzmm_plan *plan, int enable);
+
 /* Stage timing with CUDA events recorded on the execute stream (off by
    default).  Stages: 0 split + forward NTT, 1 contraction, 2 inverse NTT,
    3 CRT + recompose.  mpzmm_plan_stage_times waits for the last timed
@@ -205,6 +217,38 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
                                    const int32_t *b_sizes,
                                    uint64_t *d_c_limbs, const int64_t *c_offs,
                                    const int64_t *c_caps, int32_t *d_c_sizes, void *stream);
+
+/* ---- continuous-batching server (no counterpart in the reference) ----
+   A scheduler thread keeps up to `slots` batches in flight, each on its own
+   CUDA stream.  Whenever a slot is free it admits queued requests in arrival
+   order into one batch while their estimated device footprint fits what the
+   in-flight batches leave of `budget_bytes` (0: three quarters of the free
+   device memory), with at most `max_batch` products per batch (0: no
+   limit).  Requests that arrive while batches run join the next batch; a
+   request's residues stay on the device for the whole pipeline.  A request
+   larger than the budget is refused (MPZMM_ERR_TOO_LARGE). */
+typedef struct mpzmm_server mpzmm_server;
+MPZMM_API int mpzmm_server_create(mpzmm_server **server, int64_t budget_bytes, int slots,
+                                  int max_batch);
+/* Queues one product (host packed vectors; all arrays must stay valid until
+   the request completes) and returns its ticket. */
+MPZMM_API int mpzmm_server_submit(mpzmm_server *server, const mpzmm_product *request,
+                                  uint64_t *ticket);
+/* Waits for a ticket (timeout_ms < 0: no limit); returns the request's status
+   (MPZMM_ERR_TIMEOUT if the limit passed first). */
+MPZMM_API int mpzmm_server_wait(mpzmm_server *server, uint64_t ticket, int64_t timeout_ms);
+MPZMM_API int mpzmm_server_poll(mpzmm_server *server, uint64_t ticket, int *done);
+/* Steady-clock nanoseconds: submitted, batch launched, result written. */
+MPZMM_API int mpzmm_server_ticket_times(mpzmm_server *server, uint64_t ticket,
+                                        int64_t *submit_ns, int64_t *start_ns,
+                                        int64_t *done_ns);
+/* Forgets a completed ticket. */
+MPZMM_API int mpzmm_server_release(mpzmm_server *server, uint64_t ticket);
+/* Batches launched, products completed, most batches in flight at once. */
+MPZMM_API int mpzmm_server_stats(mpzmm_server *server, int64_t *batches, int64_t *products,
+                                 int64_t *max_in_flight);
+/* Finishes queued and in-flight work, then frees the server. */
+MPZMM_API void mpzmm_server_destroy(mpzmm_server *server);
 
 /* Parameters (prime count P, coefficient bits r, transform length 2^lgN)
    that the planner picks for a product with k terms whose A and B entries

@@ -71,6 +71,7 @@ def lib():
         "mpzmm_setup": (C.c_int, [C.c_int]),
         "mpzmm_set_option": (C.c_int, [C.c_int, C.c_int]),
         "mpzmm_get_option": (C.c_int, [C.c_int]),
+        "mpzmm_autotune": (C.c_int, [vp, C.POINTER(C.c_float)]),
         "mpzmm_last_error": (C.c_char_p, []),
         "mpzmm_device_available": (C.c_int, []),
         "mpzmm_matmul": (C.c_int, [C.c_int, C.c_int, C.c_int, u64p, i64p, i32p, u64p, i64p,
@@ -83,11 +84,20 @@ def lib():
         "mpzmm_plan_upload": (C.c_int, [vp, vp]),
         "mpzmm_plan_destroy": (None, [vp]),
         "mpzmm_plan_set_timing": (C.c_int, [vp, C.c_int]),
+        "mpzmm_plan_set_graph": (C.c_int, [vp, C.c_int]),
         "mpzmm_plan_stage_times": (C.c_int, [vp, C.POINTER(C.c_float), i64p, i64p]),
         "mpzmm_plan_info": (C.c_int, [vp, i64p, i64p, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "mpzmm_matmul_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, vp, i64p, i32p, vp, i64p,
                                            i32p, vp, i64p, i64p, vp, vp]),
+        "mpzmm_server_create": (C.c_int, [C.POINTER(vp), C.c_int64, C.c_int, C.c_int]),
+        "mpzmm_server_submit": (C.c_int, [vp, C.POINTER(Product), C.POINTER(C.c_uint64)]),
+        "mpzmm_server_wait": (C.c_int, [vp, C.c_uint64, C.c_int64]),
+        "mpzmm_server_poll": (C.c_int, [vp, C.c_uint64, C.POINTER(C.c_int)]),
+        "mpzmm_server_ticket_times": (C.c_int, [vp, C.c_uint64, i64p, i64p, i64p]),
+        "mpzmm_server_release": (C.c_int, [vp, C.c_uint64]),
+        "mpzmm_server_stats": (C.c_int, [vp, i64p, i64p, i64p]),
+        "mpzmm_server_destroy": (None, [vp]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

@@ -40,6 +40,14 @@ def set_contract_mode(mode: int) -> None:
     _lib.check(_lib.lib().mpzmm_set_option(_lib.MPZMM_OPT_CONTRACT, mode))
 
 
+def autotune(stream=None):
+    """Measure CUDA-core vs tensor-core contraction per size class; automatic
+    mode then uses the faster one.  Returns {k: (cuda_ms, tc_ms)}."""
+    ms = (C.c_float * 8)()
+    _lib.check(_lib.lib().mpzmm_autotune(_stream_arg(stream), ms))
+    return {k: (ms[2 * i], ms[2 * i + 1]) for i, k in enumerate((8, 16, 32, 64))}
+
+
 def contract_mode() -> int:
     return int(_lib.lib().mpzmm_get_option(_lib.MPZMM_OPT_CONTRACT))
 
@@ -153,6 +161,10 @@ class Plan:
         return {"launches": launches.value, "device_bytes": nbytes.value,
                 "P": P.value, "r": r.value, "lgN": lg.value}
 
+    def set_graph(self, on: bool) -> None:
+        """Capture the plan's launches into a CUDA graph on the next execute."""
+        _lib.check(_lib.lib().mpzmm_plan_set_graph(self.handle, 1 if on else 0))
+
     def set_timing(self, on: bool) -> None:
         _lib.check(_lib.lib().mpzmm_plan_set_timing(self.handle, 1 if on else 0))
 
@@ -170,6 +182,59 @@ class Plan:
         if self.handle:
             _lib.lib().mpzmm_plan_destroy(self.handle)
             self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request server (mpzmm_server_* of the C ABI)."""
+
+    def __init__(self, budget_bytes: int = 0, slots: int = 3, max_batch: int = 0):
+        self.handle = C.c_void_p()
+        _lib.check(_lib.lib().mpzmm_server_create(C.byref(self.handle), budget_bytes, slots,
+                                                  max_batch))
+        self.holders = {}
+
+    def submit(self, m: int, k: int, n: int, A: Packed, B: Packed) -> int:
+        h = _Holder(m, k, n, A, B)
+        t = C.c_uint64()
+        _lib.check(_lib.lib().mpzmm_server_submit(self.handle, C.byref(h.struct), C.byref(t)))
+        self.holders[t.value] = h
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> Packed:
+        _lib.check(_lib.lib().mpzmm_server_wait(self.handle, ticket, timeout_ms))
+        return self.holders[ticket].result()
+
+    def done(self, ticket: int) -> bool:
+        d = C.c_int()
+        _lib.check(_lib.lib().mpzmm_server_poll(self.handle, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def times(self, ticket: int):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        _lib.check(_lib.lib().mpzmm_server_ticket_times(self.handle, ticket, C.byref(a),
+                                                        C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def release(self, ticket: int) -> None:
+        _lib.check(_lib.lib().mpzmm_server_release(self.handle, ticket))
+        self.holders.pop(ticket, None)
+
+    def stats(self):
+        b, p, f = C.c_int64(), C.c_int64(), C.c_int64()
+        _lib.check(_lib.lib().mpzmm_server_stats(self.handle, C.byref(b), C.byref(p), C.byref(f)))
+        return {"batches": b.value, "products": p.value, "max_in_flight": f.value}
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.lib().mpzmm_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+            self.holders.clear()
 
     def __del__(self):
         try:

@@ -115,6 +115,7 @@ int ensure_setup(int device) {
   g_ctx.num_sms = prop.multiProcessorCount;
   const Moduli& M = moduli();
   CU(upload_constants(M.pc, &M.crt), "upload constants");
+  CU(init_kernel_attributes(), "kernel attributes");
   const size_t tw = M.twf.size();
   CU(cudaMalloc(&g_ctx.d_twf, tw * sizeof(uint2)), "cudaMalloc twiddles");
   CU(cudaMalloc(&g_ctx.d_twi, tw * sizeof(uint2)), "cudaMalloc twiddles");
@@ -150,6 +151,8 @@ void teardown() {
 
 Plan::~Plan() {
   for (cudaEvent_t e : events_) cudaEventDestroy(e);
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
 }
 
 int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
@@ -173,12 +176,16 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   auto grow_dev = [&](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
     if (*p) {
-      cudaFree(*p);
+      if (async_stream)
+        cudaFreeAsync(*p, async_stream);
+      else
+        cudaFree(*p);
       device_bytes -= (int64_t)(cap * elem);
     }
     *p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc((void**)p, want * elem);
+    cudaError_t e = async_stream ? cudaMallocAsync((void**)p, want * elem, async_stream)
+                                 : cudaMalloc((void**)p, want * elem);
     if (e != cudaSuccess) {
       *p = nullptr;
       return set_error(kErrNoMem, std::string("cudaMalloc of ") + std::to_string(want * elem) +
@@ -209,7 +216,8 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   if ((st = grow_dev(&d_sizes, cap_sizes, sizes, 4))) return st;
   if ((st = grow_dev(&d_desc, cap_desc, desc_bytes, 1))) return st;
   if (!d_status) {
-    cudaError_t e = cudaMalloc((void**)&d_status, sizeof(int));
+    cudaError_t e = async_stream ? cudaMallocAsync((void**)&d_status, sizeof(int), async_stream)
+                                 : cudaMalloc((void**)&d_status, sizeof(int));
     if (e != cudaSuccess) {
       d_status = nullptr;
       return set_error(kErrNoMem, std::string("cudaMalloc(status): ") + cudaGetErrorString(e));
@@ -223,29 +231,56 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   return kOk;
 }
 
-void Workspace::release() {
-  cudaFree(d_limbs);
-  cudaFree(d_res);
-  cudaFree(d_out);
-  cudaFree(d_sizes);
-  cudaFree(d_desc);
-  cudaFree(d_status);
-  d_status = nullptr;
-  cudaFreeHost(h_limbs);
-  cudaFreeHost(h_out);
-  cudaFreeHost(h_sizes);
-  cudaFreeHost(h_desc);
+void Workspace::release_device() {
+  for (void* p : {(void*)d_limbs, (void*)d_res, (void*)d_out, (void*)d_sizes, (void*)d_desc,
+                  (void*)d_status}) {
+    if (!p) continue;
+    if (async_stream)
+      cudaFreeAsync(p, async_stream);
+    else
+      cudaFree(p);
+  }
   d_limbs = nullptr;
   d_res = d_out = nullptr;
   d_sizes = nullptr;
   d_desc = nullptr;
+  d_status = nullptr;
+  cap_limbs = cap_res = cap_out = cap_sizes = cap_desc = 0;
+  device_bytes = 0;
+}
+
+void Workspace::release() {
+  release_device();
+  cudaFreeHost(h_limbs);
+  cudaFreeHost(h_out);
+  cudaFreeHost(h_sizes);
+  cudaFreeHost(h_desc);
   h_limbs = nullptr;
   h_out = nullptr;
   h_sizes = nullptr;
   h_desc = nullptr;
-  cap_limbs = cap_res = cap_out = cap_sizes = cap_desc = 0;
   hcap_limbs = hcap_out = hcap_sizes = hcap_desc = 0;
-  device_bytes = 0;
+}
+
+int64_t estimate_device_bytes(const ProductSpec& ps) {
+  int64_t a_bits = 0, b_bits = 0, limbs = 0;
+  for (const auto& e : ps.a) {
+    const int64_t b = bit_length(e);
+    if (b > a_bits) a_bits = b;
+    limbs += e.size < 0 ? -(int64_t)e.size : e.size;
+  }
+  for (const auto& e : ps.b) {
+    const int64_t b = bit_length(e);
+    if (b > b_bits) b_bits = b;
+    limbs += e.size < 0 ? -(int64_t)e.size : e.size;
+  }
+  Params prm;
+  if (!choose_params(a_bits, b_bits, ps.m, ps.k, ps.n, &prm)) return -1;
+  const int64_t entries = (int64_t)ps.m * ps.k + (int64_t)ps.k * ps.n + (int64_t)ps.m * ps.n;
+  const int64_t res = prm.P ? entries * prm.P * ((int64_t)1 << prm.lgN) * 4 : 0;
+  const int64_t out = (int64_t)ps.m * ps.n * prm.out_limbs * 8;
+  const int64_t desc = entries * 64 + 4096;
+  return limbs * 8 + res + out + desc;
 }
 
 int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
@@ -336,7 +371,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     pd_.push_back(pd);
     const int mode = context().contract_mode;
     const bool use_tc = contract_tc_eligible(m, k, n) &&
-                        (mode == 2 || (mode == 0 && k >= kTcMinK));
+                        (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket(k)] == 1));
     if (use_tc) {
       if (k > tc_max_k_) tc_max_k_ = k;
       if (n > tc_max_n_) tc_max_n_ = n;
@@ -521,9 +556,28 @@ int Plan::upload(cudaStream_t st) {
 
 int Plan::execute(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
+  if (!use_graph_ || timing_) return launch_all(st, timing_);
+  if (!graph_exec_) {
+    CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    const int rc = launch_all(st, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    graph_ = g;
+    CU(cudaGraphInstantiate(&graph_exec_, graph_, 0), "cudaGraphInstantiate");
+  }
+  CU(cudaGraphLaunch(graph_exec_, st), "cudaGraphLaunch");
+  return kOk;
+}
+
+int Plan::launch_all(cudaStream_t st, bool timed) {
   const Context& ctx = context();
   cudaEvent_t ev[kStages + 1] = {};
-  if (timing_) {
+  if (timed) {
     for (auto& e : ev) {
       CU(cudaEventCreate(&e), "cudaEventCreate");
       events_.push_back(e);
@@ -540,14 +594,14 @@ int Plan::execute(cudaStream_t st) {
                           ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
          "split+forward NTT launch");
   }
-  if (timing_) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
+  if (timed) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
   if (!tc_items_.empty())
     CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, kTcFreqsPerCta,
                           tc_max_k_, tc_max_n_, ws_->d_status, st),
        "tensor-core contraction launch");
-  if (timing_) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
+  if (timed) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
   for (const Group& g : inv_groups_) {
     if (g.batched)
       CU(launch_inv_items(d_inv_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.team,
@@ -558,12 +612,12 @@ int Plan::execute(cudaStream_t st) {
                         ctx.d_twi, st),
          "inverse NTT launch");
   }
-  if (timing_) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
+  if (timed) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
   for (const Group& g : rec_groups_)
     CU(launch_crt_recompose(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, ws_->d_res,
                             ws_->d_out, ws_->d_sizes, g.max_r, st),
        "CRT+recompose launch");
-  if (timing_) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
+  if (timed) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
   return kOk;
 }
 

@@ -69,11 +69,19 @@ struct Workspace {
   size_t cap_limbs = 0, cap_res = 0, cap_out = 0, cap_sizes = 0, cap_desc = 0;
   size_t hcap_limbs = 0, hcap_out = 0, hcap_sizes = 0, hcap_desc = 0;
   int64_t device_bytes = 0;
+  // With a stream set, device buffers come from the stream-ordered memory
+  // pool (cudaMallocAsync / cudaFreeAsync on that stream).
+  cudaStream_t async_stream = nullptr;
   // Ensures room for the given element counts; returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes);
+  void release_device();  // device buffers only (pinned host buffers stay)
   void release();
   ~Workspace() { release(); }
 };
+
+// Device bytes a batch of products will reserve (parameters, residues,
+// limbs, outputs and descriptors), without building it.
+int64_t estimate_device_bytes(const ProductSpec& ps);
 
 // Process-wide device state: tables on the device, default stream.
 struct Context {
@@ -87,11 +95,18 @@ struct Context {
   // contraction engine: 0 automatic (tensor cores from kTcMinK terms on),
   // 1 CUDA cores only, 2 tensor cores wherever the shape allows
   int contract_mode = 0;
+  // measured engine choice per term-count bucket (ceil(log2 k) <= 3, 4, 5, 6)
+  // in automatic mode: -1 not measured (CUDA cores), 0 CUDA cores, 1 tensor
+  // cores; filled by mpzmm_autotune
+  int tc_pref[4] = {-1, -1, -1, -1};
 };
 
-// Products with at least this many terms use the tensor-core contraction in
-// automatic mode (below it the byte split costs more than it saves).
-constexpr int kTcMinK = 24;
+inline int tc_bucket(int k) {
+  int b = 0;
+  while ((1 << (b + 3)) < k) ++b;
+  return b < 4 ? b : 3;
+}
+
 constexpr int kTcFreqsPerCta = 16;
 
 Context& context();
@@ -113,8 +128,11 @@ class Plan {
   // Gathers input limbs into pinned memory and copies them (and the
   // descriptors) to the device.
   int upload(cudaStream_t st);
-  // Runs split+fwd NTT, contraction, inverse NTT, CRT+recompose.
+  // Runs split+fwd NTT, contraction, inverse NTT, CRT+recompose.  With
+  // graph mode on (and timing off) the launches are captured into a CUDA
+  // graph on the first call and replayed as one graph launch afterwards.
   int execute(cudaStream_t st);
+  void set_graph(bool on) { use_graph_ = on; }
   // Copies outputs back and writes them to the output references.
   int download(cudaStream_t st);
 
@@ -177,6 +195,10 @@ class Plan {
   bool built_ = false;
   bool timing_ = false;
   std::vector<cudaEvent_t> events_;  // kStages + 1 per timed execute
+  bool use_graph_ = false;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int launch_all(cudaStream_t st, bool timed);
 };
 
 }  // namespace mpzmm

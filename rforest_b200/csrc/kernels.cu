@@ -798,18 +798,8 @@ static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
   const size_t smem = team ? sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5))
                            : sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
   if (team) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     k_fwd2<D, true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
   } else {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     k_fwd2<D, false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
   }
   return cudaGetLastError();
@@ -841,18 +831,8 @@ cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const Ct
   const size_t smem = team ? sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5))
                            : sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
   if (team) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_inv2<true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     k_inv2<true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, res, twi);
   } else {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_inv2<false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
     k_inv2<false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, res, twi);
   }
   return cudaGetLastError();
@@ -863,11 +843,6 @@ cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int coun
                              const uint2* twf, cudaStream_t st) {
   if (count == 0) return cudaSuccess;
   const size_t smem = sizeof(uint32_t) << lgN;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-  }
   dim3 grid(count, P);
   k_split_fwd<<<grid, ntt_threads(lgN), smem, st>>>(descs, idx, limbs, res, twf);
   return cudaGetLastError();
@@ -877,11 +852,6 @@ cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count,
                            int lgN, uint32_t* res, const uint2* twi, cudaStream_t st) {
   if (count == 0) return cudaSuccess;
   const size_t smem = sizeof(uint32_t) << lgN;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-  }
   dim3 grid(count, P);
   k_inv_ntt<<<grid, ntt_threads(lgN), smem, st>>>(descs, idx, res, twi);
   return cudaGetLastError();
@@ -909,9 +879,6 @@ cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items,
   size_t smem = (128 + ncols) * kprime;
   // at least 120 KB so that one CTA (512 TMEM columns) runs per SM
   if (smem < 120 * 1024) smem = 120 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
   k_contract_tc<<<count, tc::kThreads, smem, st>>>(prods, items, res, fb, status);
   return cudaGetLastError();
 }
@@ -924,11 +891,6 @@ static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int c
   const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P);
   const size_t smem = per_warp * kCrtWarps;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_crt_warp<P>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
   const int grid = (count + kCrtWarps - 1) / kCrtWarps;
   k_crt_warp<P><<<grid, 32 * kCrtWarps, smem, st>>>(descs, idx, count, res, out, sizes, cmax);
   return cudaGetLastError();
@@ -962,6 +924,58 @@ cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int 
     default:
       return cudaErrorInvalidValue;
   }
+}
+
+
+// Dynamic shared memory limits of every kernel, set once per device at
+// set-up (so that launches, including those captured into a CUDA graph,
+// issue nothing but stream work).
+template <int D>
+static cudaError_t set_fwd_attrs() {
+  const int big = (int)(sizeof(uint32_t) * ((1 << kMaxLgN) + ((1 << kMaxLgN) >> 5)));
+  cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fwd2<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+}
+
+template <int P>
+static cudaError_t set_crt_attr() {
+  return cudaFuncSetAttribute(k_crt_warp<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              200 * 1024);
+}
+
+cudaError_t init_kernel_attributes() {
+  cudaError_t e;
+  const int big = (int)(sizeof(uint32_t) * ((1 << kMaxLgN) + ((1 << kMaxLgN) >> 5)));
+  if ((e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(uint32_t) << kMaxLgN))) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(uint32_t) << kMaxLgN))) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_inv2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_inv2<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) !=
+      cudaSuccess)
+    return e;
+  if ((e = set_fwd_attrs<1>()) != cudaSuccess || (e = set_fwd_attrs<2>()) != cudaSuccess ||
+      (e = set_fwd_attrs<3>()) != cudaSuccess || (e = set_fwd_attrs<4>()) != cudaSuccess ||
+      (e = set_fwd_attrs<5>()) != cudaSuccess || (e = set_fwd_attrs<6>()) != cudaSuccess ||
+      (e = set_fwd_attrs<7>()) != cudaSuccess)
+    return e;
+  if ((e = set_crt_attr<2>()) != cudaSuccess || (e = set_crt_attr<3>()) != cudaSuccess ||
+      (e = set_crt_attr<4>()) != cudaSuccess || (e = set_crt_attr<5>()) != cudaSuccess ||
+      (e = set_crt_attr<6>()) != cudaSuccess || (e = set_crt_attr<7>()) != cudaSuccess ||
+      (e = set_crt_attr<8>()) != cudaSuccess || (e = set_crt_attr<9>()) != cudaSuccess ||
+      (e = set_crt_attr<10>()) != cudaSuccess || (e = set_crt_attr<11>()) != cudaSuccess ||
+      (e = set_crt_attr<12>()) != cudaSuccess || (e = set_crt_attr<13>()) != cudaSuccess ||
+      (e = set_crt_attr<14>()) != cudaSuccess || (e = set_crt_attr<15>()) != cudaSuccess ||
+      (e = set_crt_attr<16>()) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(k_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((128 + 8 * tc::kMaxN) * 4 * tc::kMaxK));
 }
 
 }  // namespace mpzmm

@@ -8,6 +8,8 @@
 namespace mpzmm {
 
 cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt);
+// Sets every kernel's dynamic shared-memory limit on the current device.
+cudaError_t init_kernel_attributes();
 
 // Radix-2 split + forward NTT / inverse NTT, one CTA per (entry, prime),
 // for `count` entries of one class (any lgN >= 1; used for lgN < 3).

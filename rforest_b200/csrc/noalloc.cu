@@ -76,6 +76,7 @@ int setup_device(int dev, DeviceState** out) {
       return cufail(e, "cudaGetSymbolAddress(twiddles)");
     const Moduli& M = moduli();
     if ((e = upload_constants(M.pc, &M.crt)) != cudaSuccess) return cufail(e, "constants");
+    if ((e = init_kernel_attributes()) != cudaSuccess) return cufail(e, "kernel attributes");
     if ((e = cudaMemcpy(s.twf, M.twf.data(), sizeof(uint2) * M.twf.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(s.twi, M.twi.data(), sizeof(uint2) * M.twi.size(),

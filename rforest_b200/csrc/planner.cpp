@@ -6,6 +6,7 @@
 // parameter choice is integer-only with an explicit exactness bound.
 #include "planner.h"
 
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -206,10 +207,20 @@ bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* 
   }
   const Moduli& M = moduli();
   const int clk = ceil_log2((uint64_t)k);
+  // optional limits on the prime count (tuning experiments)
+  static const int pmin_env = [] {
+    const char* e = std::getenv("MPZMM_PMIN");
+    return e ? std::atoi(e) : 2;
+  }();
+  static const int pmax_env = [] {
+    const char* e = std::getenv("MPZMM_PMAX");
+    return e ? std::atoi(e) : kMaxPrimes;
+  }();
   const int64_t nfwd = (int64_t)m * k + (int64_t)k * n;
   const int64_t ninv = (int64_t)m * n;
   int64_t best = -1;
   for (int P = 2; P <= kMaxPrimes; ++P) {
+    if (P < pmin_env || P > pmax_env) continue;
     const int budget = M.mbits[P] - 2 - clk;  // 2r + ceil(log2 minlen) <= budget
     if (budget < 3) continue;
     int r = budget / 2;

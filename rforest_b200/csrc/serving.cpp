@@ -1,0 +1,337 @@
+// Continuous-batching request server (mpzmm_server_* in include/mpzmm_b200.h).
+//
+// Callers submit single products from any thread; a scheduler thread owns the
+// GPU work.  It keeps up to `slots` batches in flight, each on its own CUDA
+// stream with its own stream-ordered workspace.  Whenever a slot is free it
+// admits queued requests in arrival order into a new batch while their
+// estimated device footprint fits what the in-flight batches leave of the
+// device-memory budget, plans the batch (one launch per stage), copies its
+// inputs, launches it and records an event; batches finishing are copied
+// back and their requests completed.  So requests that arrive while others
+// are on the GPU join the next batch as soon as a slot and memory are free,
+// and batches on different slots overlap on the device.  No call inside the
+// scheduler waits on the device except the copy-back of a batch whose event
+// has already completed.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mpzmm_b200.h"
+#include "engine.h"
+
+using namespace mpzmm;
+
+namespace {
+
+int64_t now_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+struct Ticket {
+  uint64_t id = 0;
+  ProductSpec spec;
+  int64_t bytes = 0;
+  int64_t t_submit = 0, t_start = 0, t_done = 0;
+  int status = -1;  // -1 pending
+  std::string error;
+};
+
+struct Slot {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  Workspace ws;
+  std::unique_ptr<Plan> plan;
+  std::vector<std::shared_ptr<Ticket>> tickets;
+  int64_t bytes = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+struct mpzmm_server {
+  int64_t budget = 0;
+  int max_batch = 0;
+  std::vector<std::unique_ptr<Slot>> slots;
+  std::mutex mu;
+  std::condition_variable cv_work;  // scheduler wakes up
+  std::condition_variable cv_done;  // waiters wake up
+  std::deque<std::shared_ptr<Ticket>> queue;
+  std::unordered_map<uint64_t, std::shared_ptr<Ticket>> tickets;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread thread;
+  int64_t in_flight_bytes = 0;
+  int64_t stat_batches = 0, stat_products = 0, stat_max_in_flight = 0;
+
+  void complete(const std::shared_ptr<Ticket>& t, int status, const std::string& err) {
+    t->status = status;
+    t->error = err;
+    t->t_done = now_ns();
+  }
+
+  // Launches one admitted batch on a free slot (scheduler thread, lock not held).
+  void launch(Slot& s, std::vector<std::shared_ptr<Ticket>> batch, int64_t bytes) {
+    std::vector<ProductSpec> specs;
+    specs.reserve(batch.size());
+    for (auto& t : batch) specs.push_back(t->spec);
+    s.plan.reset(new Plan);
+    int st = s.plan->build(std::move(specs), &s.ws);
+    if (!st) st = s.plan->upload(s.stream);
+    if (!st) st = s.plan->execute(s.stream);
+    if (!st) {
+      const cudaError_t e = cudaEventRecord(s.done, s.stream);
+      if (e != cudaSuccess) st = set_error(kErrCuda, cudaGetErrorString(e));
+    }
+    const int64_t t0 = now_ns();
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& t : batch) t->t_start = t0;
+    if (st) {
+      const std::string err = last_error();
+      for (auto& t : batch) complete(t, st, err);
+      in_flight_bytes -= bytes;
+      s.plan.reset();
+      s.ws.release_device();
+      cv_done.notify_all();
+      return;
+    }
+    s.tickets = std::move(batch);
+    s.bytes = bytes;
+    s.busy = true;
+    ++stat_batches;
+  }
+
+  // Copies back a finished batch and completes its tickets.
+  void finish(Slot& s) {
+    const int st = s.plan->download(s.stream);
+    const std::string err = st ? last_error() : std::string();
+    s.plan.reset();
+    s.ws.release_device();  // back to the stream-ordered pool
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& t : s.tickets) complete(t, st, err);
+    stat_products += (int64_t)s.tickets.size();
+    in_flight_bytes -= s.bytes;
+    s.tickets.clear();
+    s.bytes = 0;
+    s.busy = false;
+    cv_done.notify_all();
+  }
+
+  void run() {
+    cudaSetDevice(context().device);
+    for (;;) {
+      bool progressed = false;
+      // completions
+      for (auto& sp : slots) {
+        Slot& s = *sp;
+        if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+          finish(s);
+          progressed = true;
+        }
+      }
+      // admissions
+      for (auto& sp : slots) {
+        Slot& s = *sp;
+        if (s.busy) continue;
+        std::vector<std::shared_ptr<Ticket>> batch;
+        int64_t bytes = 0;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          int busy_slots = 0;
+          for (auto& o : slots) busy_slots += o->busy ? 1 : 0;
+          while (!queue.empty() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
+            const auto& t = queue.front();
+            const bool fits = in_flight_bytes + bytes + t->bytes <= budget;
+            // a request larger than the free budget still runs once the GPU
+            // is otherwise idle (admitting alone), as long as it fits at all
+            const bool alone = batch.empty() && busy_slots == 0 && in_flight_bytes == 0 &&
+                               t->bytes <= budget;
+            if (!fits && !alone) break;
+            bytes += t->bytes;
+            batch.push_back(t);
+            queue.pop_front();
+            if (!fits) break;
+          }
+          if (!batch.empty()) {
+            in_flight_bytes += bytes;
+            int in_flight = 1;
+            for (auto& o : slots) in_flight += o->busy ? 1 : 0;
+            if (in_flight > stat_max_in_flight) stat_max_in_flight = in_flight;
+          }
+        }
+        if (!batch.empty()) {
+          launch(s, std::move(batch), bytes);
+          progressed = true;
+        }
+      }
+      std::unique_lock<std::mutex> lk(mu);
+      bool any_busy = false;
+      for (auto& sp : slots) any_busy |= sp->busy;
+      if (stop && queue.empty() && !any_busy) break;
+      if (!progressed) {
+        if (any_busy)
+          cv_work.wait_for(lk, std::chrono::microseconds(20));
+        else
+          cv_work.wait_for(lk, std::chrono::milliseconds(5),
+                           [&] { return stop || !queue.empty(); });
+      }
+    }
+  }
+};
+
+extern "C" {
+
+int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int max_batch) {
+  if (!out) return set_error(kErrArg, "null server pointer");
+  *out = nullptr;
+  if (slots < 1 || slots > 16) return set_error(kErrArg, "slots must be in 1..16");
+  int st = ensure_setup(-1);
+  if (st) return st;
+  std::unique_ptr<mpzmm_server> s(new mpzmm_server);
+  if (budget_bytes <= 0) {
+    size_t fr = 0, tot = 0;
+    const cudaError_t e = cudaMemGetInfo(&fr, &tot);
+    if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
+    budget_bytes = (int64_t)(fr / 4 * 3);
+  }
+  s->budget = budget_bytes;
+  s->max_batch = max_batch;
+  // keep freed pool memory cached for the next batch
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, context().device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  for (int i = 0; i < slots; ++i) {
+    std::unique_ptr<Slot> sl(new Slot);
+    cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
+    sl->ws.async_stream = sl->stream;
+    s->slots.push_back(std::move(sl));
+  }
+  mpzmm_server* raw = s.get();
+  s->thread = std::thread([raw] { raw->run(); });
+  *out = s.release();
+  return kOk;
+}
+
+int mpzmm_server_submit(mpzmm_server* s, const mpzmm_product* req, uint64_t* ticket) {
+  if (!s || !req || !ticket) return set_error(kErrArg, "null argument");
+  auto t = std::make_shared<Ticket>();
+  const mpzmm_product& p = *req;
+  if (p.m < 0 || p.k < 0 || p.n < 0) return set_error(kErrArg, "negative dimension");
+  t->spec.m = p.m;
+  t->spec.k = p.k;
+  t->spec.n = p.n;
+  const int64_t na = (int64_t)p.m * p.k, nb = (int64_t)p.k * p.n, nc = (int64_t)p.m * p.n;
+  t->spec.a.resize(na);
+  t->spec.b.resize(nb);
+  t->spec.c.resize(nc);
+  for (int64_t e = 0; e < na; ++e)
+    t->spec.a[e] = EntryRef{p.a_sizes[e] ? p.a_limbs + p.a_offs[e] : nullptr, p.a_sizes[e]};
+  for (int64_t e = 0; e < nb; ++e)
+    t->spec.b[e] = EntryRef{p.b_sizes[e] ? p.b_limbs + p.b_offs[e] : nullptr, p.b_sizes[e]};
+  for (int64_t e = 0; e < nc; ++e)
+    t->spec.c[e] = OutRef{p.c_limbs + p.c_offs[e], p.c_caps[e], p.c_sizes + e, nullptr};
+  t->bytes = estimate_device_bytes(t->spec);
+  if (t->bytes < 0) return set_error(kErrTooLarge, "product too large for a single transform");
+  if (t->bytes > s->budget)
+    return set_error(kErrTooLarge, "request needs " + std::to_string(t->bytes) +
+                                       " device bytes, the server budget is " +
+                                       std::to_string(s->budget));
+  t->t_submit = now_ns();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return set_error(kErrState, "server is stopping");
+    t->id = s->next_id++;
+    s->tickets[t->id] = t;
+    s->queue.push_back(t);
+  }
+  s->cv_work.notify_one();
+  *ticket = t->id;
+  return kOk;
+}
+
+int mpzmm_server_poll(mpzmm_server* s, uint64_t ticket, int* done) {
+  if (!s || !done) return set_error(kErrArg, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return set_error(kErrArg, "unknown ticket");
+  *done = it->second->status >= 0 ? 1 : 0;
+  return kOk;
+}
+
+int mpzmm_server_wait(mpzmm_server* s, uint64_t ticket, int64_t timeout_ms) {
+  if (!s) return set_error(kErrArg, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return set_error(kErrArg, "unknown ticket");
+  std::shared_ptr<Ticket> t = it->second;
+  auto ready = [&] { return t->status >= 0; };
+  if (timeout_ms < 0) {
+    s->cv_done.wait(lk, ready);
+  } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+    return set_error(kErrTimeout, "request not finished within the time limit");
+  }
+  if (t->status) return set_error(t->status, t->error);
+  return kOk;
+}
+
+int mpzmm_server_ticket_times(mpzmm_server* s, uint64_t ticket, int64_t* submit_ns,
+                              int64_t* start_ns, int64_t* done_ns) {
+  if (!s) return set_error(kErrArg, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return set_error(kErrArg, "unknown ticket");
+  if (submit_ns) *submit_ns = it->second->t_submit;
+  if (start_ns) *start_ns = it->second->t_start;
+  if (done_ns) *done_ns = it->second->t_done;
+  return kOk;
+}
+
+int mpzmm_server_release(mpzmm_server* s, uint64_t ticket) {
+  if (!s) return set_error(kErrArg, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return set_error(kErrArg, "unknown ticket");
+  if (it->second->status < 0) return set_error(kErrState, "request still pending");
+  s->tickets.erase(it);
+  return kOk;
+}
+
+int mpzmm_server_stats(mpzmm_server* s, int64_t* batches, int64_t* products,
+                       int64_t* max_in_flight) {
+  if (!s) return set_error(kErrArg, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (batches) *batches = s->stat_batches;
+  if (products) *products = s->stat_products;
+  if (max_in_flight) *max_in_flight = s->stat_max_in_flight;
+  return kOk;
+}
+
+void mpzmm_server_destroy(mpzmm_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->thread.joinable()) s->thread.join();  // drains queued and in-flight work
+  for (auto& sl : s->slots) {
+    cudaStreamSynchronize(sl->stream);
+    sl->ws.release();
+    cudaEventDestroy(sl->done);
+    cudaStreamDestroy(sl->stream);
+  }
+  delete s;
+}
+
+}  // extern "C"

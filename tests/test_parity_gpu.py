@@ -217,3 +217,17 @@ def test_tc_config4_full_size(tensor_cores):
     C = api.matmul(64, 64, 64, p.A, p.B)
     d = G.digests()
     assert PK.digest(C) == d["config4"]["C"]
+
+
+def test_autotune_then_automatic_engine_is_exact(gpu):
+    times = api.autotune()
+    assert set(times) == {8, 16, 32, 64}
+    assert all(c > 0 and t > 0 for c, t in times.values())
+    rng = random.Random(77)
+    for (m, k, n) in [(5, 40, 7), (32, 64, 3), (2, 9, 2)]:
+        Ai = [rng.randrange(-(1 << 3000), 1 << 3000) for _ in range(m * k)]
+        Bi = [rng.randrange(-(1 << 2000), 1 << 2000) for _ in range(k * n)]
+        C = api.matmul(m, k, n, PK.from_ints(Ai), PK.from_ints(Bi))
+        want = [sum(Ai[i * k + l] * Bi[l * n + j] for l in range(k))
+                for i in range(m) for j in range(n)]
+        assert C.to_ints() == want
