@@ -432,7 +432,8 @@ def main():
                            params_product0=info, device_bytes=info["device_bytes"],
                            e2e_steps=e2e_steps, parallelism=f"replicas x{world}",
                            contract=args.contract,
-                           autotune_contract_ms={str(k): v for k, v in tuning.items()}),
+                           autotune_contract_ms={f"k{k}_mn{mn}": [round(v[0], 4), round(v[1], 4)]
+                                                 for (k, mn), v in tuning.items()}),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(stage_launches) * args.steps),

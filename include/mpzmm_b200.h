@@ -107,10 +107,11 @@ MPZMM_API int mpzmm_set_option(int option, int value);
 MPZMM_API int mpzmm_get_option(int option);
 
 /* Autotuner: times the contraction of a representative product per size
-   class (32 x k by k x 32 with k = 8, 16, 32, 64, 2^14-bit entries) on CUDA
-   cores and on tensor cores and makes automatic mode use the faster engine
-   for that class (until then automatic mode uses CUDA cores).  ms_out, if
-   not NULL, receives 8 floats: {CUDA, tensor} milliseconds per class. */
+   class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
+   entries) on CUDA cores and on tensor cores and makes automatic mode use
+   the faster engine for that class (until then automatic mode uses CUDA
+   cores).  ms_out, if not NULL, receives 40 floats: {CUDA, tensor}
+   milliseconds per class, k-major. */
 MPZMM_API int mpzmm_autotune(void *stream, float *ms_out);
 
 /* Human-readable message for the last error on the calling thread. */

@@ -42,10 +42,15 @@ def set_contract_mode(mode: int) -> None:
 
 def autotune(stream=None):
     """Measure CUDA-core vs tensor-core contraction per size class; automatic
-    mode then uses the faster one.  Returns {k: (cuda_ms, tc_ms)}."""
-    ms = (C.c_float * 8)()
+    mode then uses the faster one.  Returns {(k, m=n): (cuda_ms, tc_ms)}."""
+    ms = (C.c_float * 40)()
     _lib.check(_lib.lib().mpzmm_autotune(_stream_arg(stream), ms))
-    return {k: (ms[2 * i], ms[2 * i + 1]) for i, k in enumerate((8, 16, 32, 64))}
+    out = {}
+    for bk, k in enumerate((8, 16, 32, 64)):
+        for bm, mn in enumerate((4, 8, 16, 32, 64)):
+            i = bk * 5 + bm
+            out[(k, mn)] = (ms[2 * i], ms[2 * i + 1])
+    return out
 
 
 def contract_mode() -> int:

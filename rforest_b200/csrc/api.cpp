@@ -101,66 +101,66 @@ int mpzmm_set_option(int option, int value) {
   return set_error(kErrArg, "unknown option");
 }
 
-// Times the contraction stage of a representative product per term-count
-// bucket (32 x k by k x 32, 2^14-bit entries, k = 8, 16, 32, 64) on CUDA
-// cores and on tensor cores, and records the faster engine for automatic
-// mode.  ms_out (optional) receives {cuda, tc} milliseconds per bucket.
+// Times the contraction stage of one representative product per size class
+// (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit entries) on
+// CUDA cores and on tensor cores, and records the faster engine for
+// automatic mode.  ms_out (optional) receives {cuda, tc} milliseconds per
+// class, k-major (40 floats).
 int mpzmm_autotune(void* stream, float* ms_out) {
   int st = ensure_setup(-1);
   if (st) return st;
   cudaStream_t s = pick_stream(stream);
   const int ks[4] = {8, 16, 32, 64};
+  const int mns[5] = {4, 8, 16, 32, 64};
   const int saved = context().contract_mode;
   uint64_t x = 0x9E3779B97F4A7C15ull;
-  for (int b = 0; b < 4; ++b) {
-    const int m = 32, k = ks[b], n = 32, nl = 256;  // 2^14-bit entries
-    std::vector<uint64_t> limbs((size_t)(m * k + k * n) * nl);
-    for (auto& w : limbs) {
-      x ^= x << 13;
-      x ^= x >> 7;
-      x ^= x << 17;
-      w = x;
-    }
-    std::vector<uint64_t> out((size_t)m * n * (2 * nl + 2));
-    float ms[2] = {0.f, 0.f};
-    for (int mode = 1; mode <= 2; ++mode) {
-      ProductSpec ps;
-      ps.m = m;
-      ps.k = k;
-      ps.n = n;
-      for (int e = 0; e < m * k; ++e) ps.a.push_back(EntryRef{&limbs[(size_t)e * nl], nl});
-      for (int e = 0; e < k * n; ++e)
-        ps.b.push_back(EntryRef{&limbs[(size_t)(m * k + e) * nl], nl});
-      for (int e = 0; e < m * n; ++e)
-        ps.c.push_back(OutRef{&out[(size_t)e * (2 * nl + 2)], 2 * nl + 2, nullptr, nullptr});
-      context().contract_mode = mode;
-      Plan plan;
-      std::vector<ProductSpec> v;
-      v.push_back(std::move(ps));
-      if ((st = plan.build(std::move(v))) || (st = plan.upload(s)) || (st = plan.execute(s))) {
-        context().contract_mode = saved;
-        return st;
+  auto fail = [&](int code) {
+    context().contract_mode = saved;
+    return code;
+  };
+  for (int bk = 0; bk < 4; ++bk)
+    for (int bm = 0; bm < 5; ++bm) {
+      const int m = mns[bm], k = ks[bk], n = mns[bm], nl = 256;  // 2^14-bit entries
+      std::vector<uint64_t> limbs((size_t)(m * k + k * n) * nl);
+      for (auto& w : limbs) {
+        x ^= x << 13;
+        x ^= x >> 7;
+        x ^= x << 17;
+        w = x;
       }
-      plan.set_timing(true);
-      for (int rep = 0; rep < 3; ++rep)
-        if ((st = plan.execute(s))) {
-          context().contract_mode = saved;
-          return st;
-        }
-      float t[Plan::kStages];
-      int64_t ex = 0;
-      if ((st = plan.stage_times(t, &ex))) {
-        context().contract_mode = saved;
-        return st;
+      const int cap = 2 * nl + 2;
+      std::vector<uint64_t> out((size_t)m * n * cap);
+      float ms[2] = {0.f, 0.f};
+      for (int mode = 1; mode <= 2; ++mode) {
+        ProductSpec ps;
+        ps.m = m;
+        ps.k = k;
+        ps.n = n;
+        for (int e = 0; e < m * k; ++e) ps.a.push_back(EntryRef{&limbs[(size_t)e * nl], nl});
+        for (int e = 0; e < k * n; ++e)
+          ps.b.push_back(EntryRef{&limbs[(size_t)(m * k + e) * nl], nl});
+        for (int e = 0; e < m * n; ++e)
+          ps.c.push_back(OutRef{&out[(size_t)e * cap], cap, nullptr, nullptr});
+        context().contract_mode = mode;
+        Plan plan;
+        std::vector<ProductSpec> v;
+        v.push_back(std::move(ps));
+        if ((st = plan.build(std::move(v))) || (st = plan.upload(s)) || (st = plan.execute(s)))
+          return fail(st);
+        plan.set_timing(true);
+        for (int rep = 0; rep < 3; ++rep)
+          if ((st = plan.execute(s))) return fail(st);
+        float t[Plan::kStages];
+        int64_t ex = 0;
+        if ((st = plan.stage_times(t, &ex))) return fail(st);
+        ms[mode - 1] = ex ? t[1] / (float)ex : 0.f;
       }
-      ms[mode - 1] = ex ? t[1] / (float)ex : 0.f;
+      context().tc_pref[bk][bm] = ms[1] < ms[0] ? 1 : 0;
+      if (ms_out) {
+        ms_out[2 * (bk * 5 + bm)] = ms[0];
+        ms_out[2 * (bk * 5 + bm) + 1] = ms[1];
+      }
     }
-    context().tc_pref[b] = ms[1] < ms[0] ? 1 : 0;
-    if (ms_out) {
-      ms_out[2 * b] = ms[0];
-      ms_out[2 * b + 1] = ms[1];
-    }
-  }
   context().contract_mode = saved;
   return kOk;
 }

@@ -331,6 +331,9 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     const int P = prm.P, lgN = prm.lgN, r = prm.r;
     const uint64_t N = (uint64_t)1 << lgN;
     const uint64_t poly = (uint64_t)P * N;
+    // the contraction addresses a product's residues with 32-bit offsets
+    if (((uint64_t)m * k + (uint64_t)k * n + (uint64_t)m * n) * poly >= (1ull << 32))
+      return set_error(kErrTooLarge, "product needs more than 2^32 residue words");
     ProdDesc pd;
     pd.m = (uint16_t)m;
     pd.k = (uint16_t)k;
@@ -371,7 +374,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     pd_.push_back(pd);
     const int mode = context().contract_mode;
     const bool use_tc = contract_tc_eligible(m, k, n) &&
-                        (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket(k)] == 1));
+                        (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)][tc_bucket_mn(m, n)] == 1));
     if (use_tc) {
       if (k > tc_max_k_) tc_max_k_ = k;
       if (n > tc_max_n_) tc_max_n_ = n;

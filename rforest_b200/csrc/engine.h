@@ -95,16 +95,24 @@ struct Context {
   // contraction engine: 0 automatic (tensor cores from kTcMinK terms on),
   // 1 CUDA cores only, 2 tensor cores wherever the shape allows
   int contract_mode = 0;
-  // measured engine choice per term-count bucket (ceil(log2 k) <= 3, 4, 5, 6)
-  // in automatic mode: -1 not measured (CUDA cores), 0 CUDA cores, 1 tensor
-  // cores; filled by mpzmm_autotune
-  int tc_pref[4] = {-1, -1, -1, -1};
+  // measured engine choice per size class (term-count bucket k <= 8, 16, 32,
+  // 64 by row/column bucket max(m, n) <= 4, 8, 16, 32, 64) in automatic
+  // mode: -1 not measured (CUDA cores), 0 CUDA cores, 1 tensor cores;
+  // filled by mpzmm_autotune
+  int tc_pref[4][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1},
+                       {-1, -1, -1, -1, -1}};
 };
 
-inline int tc_bucket(int k) {
+inline int tc_bucket_k(int k) {
   int b = 0;
   while ((1 << (b + 3)) < k) ++b;
   return b < 4 ? b : 3;
+}
+inline int tc_bucket_mn(int m, int n) {
+  const int x = m > n ? m : n;
+  int b = 0;
+  while ((1 << (b + 2)) < x) ++b;
+  return b < 5 ? b : 4;
 }
 
 constexpr int kTcFreqsPerCta = 16;

@@ -167,6 +167,16 @@ __global__ void k_inv_ntt(const InvDesc* __restrict__ descs,
 // ---------------------------------------------------------------------------
 constexpr int kContractThreads = 128;
 
+// x mod p for any 64-bit x (Barrett on the high word, then REDC of the
+// reduced value times 2^32): keeps the accumulator's value, not its
+// Montgomery image, so folds can be repeated.
+__device__ __forceinline__ uint64_t fold64(uint64_t x, uint32_t p, uint32_t pinv, uint32_t mu,
+                                           uint32_t r2) {
+  // x = hi 2^32 + lo;  x mod p = REDC((x 2^-32 mod p) * 2^64 mod p)
+  const uint32_t t = redc64(x, p, pinv, mu);           // x 2^-32 mod p
+  return redc((uint64_t)t * r2, p, pinv);              // x mod p
+}
+
 template <int TI, int TJ>
 __device__ __forceinline__ void contract_tiles(const ProdDesc& d, int j, uint32_t h,
                                                uint32_t* __restrict__ res) {
@@ -174,55 +184,77 @@ __device__ __forceinline__ void contract_tiles(const ProdDesc& d, int j, uint32_
   const uint32_t p = c_primes[j].p;
   const uint32_t pinv = c_primes[j].pinv;
   const uint32_t mu = c_primes[j].mu;
-  const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
+  const uint32_t r2 = c_primes[j].r2;
+  const uint32_t stride = (uint32_t)d.P * (uint32_t)N;  // words between polynomials
   const uint64_t base = (uint64_t)j * (uint64_t)N + h;
   const uint32_t* __restrict__ A = res + d.a_res + base;
   const uint32_t* __restrict__ B = res + d.b_res + base;
   uint32_t* C = res + d.c_res + base;
   const int m = d.m, k = d.k, n = d.n;
-  const uint64_t bstep = (uint64_t)n * stride;
+  const uint32_t bstep = (uint32_t)n * stride;
   for (int i0 = 0; i0 < m; i0 += TI) {
     for (int l0 = 0; l0 < n; l0 += TJ) {
-      const uint32_t* Ap[TI];
-      const uint32_t* Bp[TJ];
+      uint32_t ao[TI], bo[TJ];  // word offsets of the tile's rows / columns
 #pragma unroll
       for (int x = 0; x < TI; ++x) {
         const int ii = (i0 + x) < m ? (i0 + x) : (m - 1);
-        Ap[x] = A + (uint64_t)ii * k * stride;
+        ao[x] = (uint32_t)ii * (uint32_t)k * stride;
       }
 #pragma unroll
       for (int y = 0; y < TJ; ++y) {
         const int ll = (l0 + y) < n ? (l0 + y) : (n - 1);
-        Bp[y] = B + (uint64_t)ll * stride;
+        bo[y] = (uint32_t)ll * stride;
       }
-      uint32_t sum[TI][TJ];
+      uint64_t acc[TI][TJ];
 #pragma unroll
       for (int x = 0; x < TI; ++x)
 #pragma unroll
-        for (int y = 0; y < TJ; ++y) sum[x][y] = 0;
-      for (int k0 = 0; k0 < k; k0 += 16) {
-        const int k1 = (k0 + 16) < k ? (k0 + 16) : k;
-        uint64_t acc[TI][TJ];
+        for (int y = 0; y < TJ; ++y) acc[x][y] = 0;
+      // acc < p + 15 p^2 < 2^64 between folds
+      int since = 0;
+      int q = 0;
+      for (; q + 4 <= k; q += 4) {
+        uint32_t av[4][TI], bv[4][TJ];
 #pragma unroll
-        for (int x = 0; x < TI; ++x)
+        for (int u = 0; u < 4; ++u) {
 #pragma unroll
-          for (int y = 0; y < TJ; ++y) acc[x][y] = 0;
-        for (int q = k0; q < k1; ++q) {
-          uint32_t av[TI], bv[TJ];
+          for (int x = 0; x < TI; ++x) av[u][x] = __ldg(A + ao[x] + (uint32_t)(q + u) * stride);
 #pragma unroll
-          for (int x = 0; x < TI; ++x) av[x] = __ldg(Ap[x] + (uint64_t)q * stride);
-#pragma unroll
-          for (int y = 0; y < TJ; ++y) bv[y] = __ldg(Bp[y] + (uint64_t)q * bstep);
+          for (int y = 0; y < TJ; ++y) bv[u][y] = __ldg(B + bo[y] + (uint32_t)(q + u) * bstep);
+        }
+        if (since + 4 > 15) {
 #pragma unroll
           for (int x = 0; x < TI; ++x)
 #pragma unroll
-            for (int y = 0; y < TJ; ++y) acc[x][y] += (uint64_t)av[x] * bv[y];
+            for (int y = 0; y < TJ; ++y) acc[x][y] = fold64(acc[x][y], p, pinv, mu, r2);
+          since = 0;
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int x = 0; x < TI; ++x)
+#pragma unroll
+            for (int y = 0; y < TJ; ++y) acc[x][y] += (uint64_t)av[u][x] * bv[u][y];
+        since += 4;
+      }
+      for (; q < k; ++q) {
+        if (since + 1 > 15) {
+#pragma unroll
+          for (int x = 0; x < TI; ++x)
+#pragma unroll
+            for (int y = 0; y < TJ; ++y) acc[x][y] = fold64(acc[x][y], p, pinv, mu, r2);
+          since = 0;
+        }
+        uint32_t av[TI], bv[TJ];
+#pragma unroll
+        for (int x = 0; x < TI; ++x) av[x] = __ldg(A + ao[x] + (uint32_t)q * stride);
+#pragma unroll
+        for (int y = 0; y < TJ; ++y) bv[y] = __ldg(B + bo[y] + (uint32_t)q * bstep);
 #pragma unroll
         for (int x = 0; x < TI; ++x)
 #pragma unroll
-          for (int y = 0; y < TJ; ++y)
-            sum[x][y] = add_mod(sum[x][y], redc64(acc[x][y], p, pinv, mu), p);
+          for (int y = 0; y < TJ; ++y) acc[x][y] += (uint64_t)av[x] * bv[y];
+        ++since;
       }
 #pragma unroll
       for (int x = 0; x < TI; ++x) {
@@ -230,7 +262,8 @@ __device__ __forceinline__ void contract_tiles(const ProdDesc& d, int j, uint32_
 #pragma unroll
         for (int y = 0; y < TJ; ++y) {
           if (l0 + y >= n) continue;
-          C[((uint64_t)(i0 + x) * n + (l0 + y)) * stride] = sum[x][y];
+          // the value times 2^-32 (the Montgomery factor the CRT removes)
+          C[(uint32_t)((i0 + x) * n + (l0 + y)) * stride] = redc64(acc[x][y], p, pinv, mu);
         }
       }
     }
@@ -342,7 +375,7 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
 }
 
 template <int D, bool TEAM>
-__global__ void __launch_bounds__(kFwdThreads)
+__global__ void __launch_bounds__(kFwdThreads, 3)
 k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
        const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
        uint32_t* __restrict__ res, const uint2* __restrict__ twf) {

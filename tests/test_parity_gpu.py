@@ -221,7 +221,7 @@ def test_tc_config4_full_size(tensor_cores):
 
 def test_autotune_then_automatic_engine_is_exact(gpu):
     times = api.autotune()
-    assert set(times) == {8, 16, 32, 64}
+    assert len(times) == 20 and (64, 64) in times
     assert all(c > 0 and t > 0 for c, t in times.values())
     rng = random.Random(77)
     for (m, k, n) in [(5, 40, 7), (32, 64, 3), (2, 9, 2)]:
