@@ -584,6 +584,7 @@ def serving_benchmark(api, args):
                          "p99_ms": _pct(lat, 99), "unit": "requests/s"})
         out["runs"] = runs
         out["server"] = srv.stats()
+        out["server_phase_ms"] = srv.phase_ms()
     finally:
         srv.close()
     return out

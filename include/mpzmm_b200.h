@@ -248,6 +248,9 @@ MPZMM_API int mpzmm_server_release(mpzmm_server *server, uint64_t ticket);
 /* Batches launched, products completed, most batches in flight at once. */
 MPZMM_API int mpzmm_server_stats(mpzmm_server *server, int64_t *batches, int64_t *products,
                                  int64_t *max_in_flight);
+/* Scheduler-thread nanoseconds spent in: plan building, input gather and
+   copy, kernel launches, result copy-back and scatter (4 values). */
+MPZMM_API int mpzmm_server_phase_ns(mpzmm_server *server, int64_t *ns4);
 /* Finishes queued and in-flight work, then frees the server. */
 MPZMM_API void mpzmm_server_destroy(mpzmm_server *server);
 

@@ -98,6 +98,7 @@ def lib():
         "mpzmm_server_release": (C.c_int, [vp, C.c_uint64]),
         "mpzmm_server_stats": (C.c_int, [vp, i64p, i64p, i64p]),
         "mpzmm_server_destroy": (None, [vp]),
+        "mpzmm_server_phase_ns": (C.c_int, [vp, i64p]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

@@ -235,6 +235,11 @@ class Server:
         _lib.check(_lib.lib().mpzmm_server_stats(self.handle, C.byref(b), C.byref(p), C.byref(f)))
         return {"batches": b.value, "products": p.value, "max_in_flight": f.value}
 
+    def phase_ms(self):
+        ns = (C.c_int64 * 4)()
+        _lib.check(_lib.lib().mpzmm_server_phase_ns(self.handle, C.cast(ns, _lib.i64p)))
+        return dict(zip(("build", "upload", "launch", "download"), [x / 1e6 for x in ns]))
+
     def close(self) -> None:
         if self.handle:
             _lib.lib().mpzmm_server_destroy(self.handle)

@@ -173,8 +173,15 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
                                       " free");
   }
   int st;
+  // geometric growth: a workspace serving batches of varying size settles
+  // after a few growths instead of re-allocating for every new maximum
+  auto grown = [](size_t want, size_t cap) {
+    const size_t g = cap + cap / 2;
+    return want > g ? want : g;
+  };
   auto grow_dev = [&](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
+    const size_t geo = cap ? grown(want, cap) : want;
     if (*p) {
       if (async_stream)
         cudaFreeAsync(*p, async_stream);
@@ -184,8 +191,17 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
     }
     *p = nullptr;
     cap = 0;
-    cudaError_t e = async_stream ? cudaMallocAsync((void**)p, want * elem, async_stream)
-                                 : cudaMalloc((void**)p, want * elem);
+    auto alloc = [&](size_t count) {
+      return async_stream ? cudaMallocAsync((void**)p, count * elem, async_stream)
+                          : cudaMalloc((void**)p, count * elem);
+    };
+    cudaError_t e = alloc(geo);
+    if (e != cudaSuccess && geo != want) {  // the larger size did not fit: exact size
+      cudaGetLastError();
+      e = alloc(want);
+    } else {
+      want = geo;
+    }
     if (e != cudaSuccess) {
       *p = nullptr;
       return set_error(kErrNoMem, std::string("cudaMalloc of ") + std::to_string(want * elem) +
@@ -197,6 +213,7 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   };
   auto grow_host = [&](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
+    if (cap) want = grown(want, cap);
     if (*p) cudaFreeHost(*p);
     *p = nullptr;
     cap = 0;

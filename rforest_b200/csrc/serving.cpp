@@ -2,7 +2,7 @@
 //
 // Callers submit single products from any thread; a scheduler thread owns the
 // GPU work.  It keeps up to `slots` batches in flight, each on its own CUDA
-// stream with its own stream-ordered workspace.  Whenever a slot is free it
+// stream with its own grow-only workspace.  Whenever a slot is free it
 // admits queued requests in arrival order into a new batch while their
 // estimated device footprint fits what the in-flight batches leave of the
 // device-memory budget, plans the batch (one launch per stage), copies its
@@ -70,6 +70,9 @@ struct mpzmm_server {
   std::thread thread;
   int64_t in_flight_bytes = 0;
   int64_t stat_batches = 0, stat_products = 0, stat_max_in_flight = 0;
+  // scheduler-thread time per phase (ns): plan build, input gather + copy,
+  // launches, result copy-back + scatter
+  int64_t ns_build = 0, ns_upload = 0, ns_launch = 0, ns_download = 0;
 
   void complete(const std::shared_ptr<Ticket>& t, int status, const std::string& err) {
     t->status = status;
@@ -83,14 +86,20 @@ struct mpzmm_server {
     specs.reserve(batch.size());
     for (auto& t : batch) specs.push_back(t->spec);
     s.plan.reset(new Plan);
+    const int64_t a0 = now_ns();
     int st = s.plan->build(std::move(specs), &s.ws);
+    const int64_t a1 = now_ns();
     if (!st) st = s.plan->upload(s.stream);
+    const int64_t a2 = now_ns();
     if (!st) st = s.plan->execute(s.stream);
     if (!st) {
       const cudaError_t e = cudaEventRecord(s.done, s.stream);
       if (e != cudaSuccess) st = set_error(kErrCuda, cudaGetErrorString(e));
     }
     const int64_t t0 = now_ns();
+    ns_build += a1 - a0;
+    ns_upload += a2 - a1;
+    ns_launch += t0 - a2;
     std::lock_guard<std::mutex> lk(mu);
     for (auto& t : batch) t->t_start = t0;
     if (st) {
@@ -110,10 +119,14 @@ struct mpzmm_server {
 
   // Copies back a finished batch and completes its tickets.
   void finish(Slot& s) {
+    const int64_t d0 = now_ns();
     const int st = s.plan->download(s.stream);
+    ns_download += now_ns() - d0;
     const std::string err = st ? last_error() : std::string();
     s.plan.reset();
-    s.ws.release_device();  // back to the stream-ordered pool
+    // workspaces are grow-only (re-growing per batch costs far more than the
+    // batch); one that has grown past its share of the budget is released
+    if (s.ws.device_bytes > budget / (int64_t)slots.size()) s.ws.release_device();
     std::lock_guard<std::mutex> lk(mu);
     for (auto& t : s.tickets) complete(t, st, err);
     stat_products += (int64_t)s.tickets.size();
@@ -203,18 +216,11 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
   }
   s->budget = budget_bytes;
   s->max_batch = max_batch;
-  // keep freed pool memory cached for the next batch
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, context().device) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
   for (int i = 0; i < slots; ++i) {
     std::unique_ptr<Slot> sl(new Slot);
     cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming);
     if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
-    sl->ws.async_stream = sl->stream;
     s->slots.push_back(std::move(sl));
   }
   mpzmm_server* raw = s.get();
@@ -304,6 +310,16 @@ int mpzmm_server_release(mpzmm_server* s, uint64_t ticket) {
   if (it == s->tickets.end()) return set_error(kErrArg, "unknown ticket");
   if (it->second->status < 0) return set_error(kErrState, "request still pending");
   s->tickets.erase(it);
+  return kOk;
+}
+
+int mpzmm_server_phase_ns(mpzmm_server* s, int64_t* ns4) {
+  if (!s || !ns4) return set_error(kErrArg, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  ns4[0] = s->ns_build;
+  ns4[1] = s->ns_upload;
+  ns4[2] = s->ns_launch;
+  ns4[3] = s->ns_download;
   return kOk;
 }
 
