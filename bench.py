@@ -305,18 +305,17 @@ def main():
     import torch.distributed as dist
     from rforest_b200 import api, packed as PK
 
+    from rforest_b200 import replicas
     torch.cuda.set_device(local_rank)
     if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+        replicas.init("nccl", rank, world, device=torch.device("cuda", local_rank))
     api.setup(local_rank)
     modes = {"auto": 0, "cuda": 1, "tc": 2}
     api.set_contract_mode(modes[args.contract])
     stream = torch.cuda.Stream()
     tuning = api.autotune(stream)
 
-    replicate = 1 + rank
+    replicate = replicas.replicate_of(rank)
     prods = make_workload(args.workload, replicate, args.count)
     units_per_rank = len(prods)
     triples = [(p.m, p.k, p.n, p.A, p.B) for p in prods]
@@ -345,11 +344,9 @@ def main():
     ms = ev0.elapsed_time(ev1)
     stage_ms, stage_launches, timed = plan.stage_times()
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = replicas.max_over_ranks(ms, device=torch.device("cuda", local_rank))
         dist.barrier()
-    value = units_per_rank * world * args.steps / (ms / 1000.0)
+    value = replicas.whole_job_rate(units_per_rank, world, args.steps, ms)
 
     # the same plan replayed as one CUDA graph per step
     plan.set_graph(True)
@@ -380,10 +377,8 @@ def main():
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1000.0
     if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = units_per_rank * world * e2e_steps / (e2e_ms / 1000.0)
+        e2e_ms = replicas.max_over_ranks(e2e_ms, device=torch.device("cuda", local_rank))
+    e2e_value = replicas.whole_job_rate(units_per_rank, world, e2e_steps, e2e_ms)
     h2d = sum(int(p.A.nlimbs.sum() + p.B.nlimbs.sum()) * 8 for p in prods)
     d2h_words = 0
     for p in prods:
@@ -396,7 +391,7 @@ def main():
         serving = serving_benchmark(api, args)
 
     comparisons = None
-    if not args.no_compare and args.workload == "config3":
+    if world == 1 and not args.no_compare and args.workload == "config3":
         comparisons = compare_forms(api, torch, stream, triples, args)
         api.set_contract_mode(modes[args.contract])
 
