@@ -435,12 +435,13 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   if (out_entry > 0x7fffffffULL) return set_error(kErrTooLarge, "too many output entries");
 
   // launch groups and the shared index array
-  // Transforms: size classes with lgN >= 3 are merged into one launch per
-  // kernel variant (team or not, digits D), CTA work items carrying the
-  // class; the largest classes come first so the long CTAs start early.
+  // Transforms: team-sized classes (lgN >= 3) are merged into one launch per
+  // digit count D, larger classes get one launch per (lgN, D); CTA work items
+  // carry the class, and the largest classes come first so the long CTAs
+  // start early.
   auto batch_classes = [&](std::map<std::pair<int, int>, Group>& classes, bool fwd,
                            std::vector<Group>& out) {
-    std::map<std::pair<int, int>, Group> var;
+    std::map<std::pair<int, int>, Group> var;  // (0 = team, else lgN; D)
     for (auto& kv : classes) {
       Group& g = kv.second;
       const int D = fwd ? (g.max_r + 29) / 30 : 0;
@@ -449,7 +450,9 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
         continue;
       }
       const bool team = ((int64_t)1 << g.lgN) <= (int64_t)fwd_team_points();
-      Group& v = var[{team ? 1 : 0, D}];
+      // a CTA's shared memory follows the launch's largest class, so classes
+      // above the team size get launches of their own
+      Group& v = var[{team ? 0 : g.lgN, D}];
       v.batched = true;
       v.team = team;
       v.D = D;
