@@ -101,10 +101,34 @@ MPZMM_API int mpzmm_setup(int device);
    0 automatic (per size class, the engine mpzmm_autotune measured faster;
    tensor cores -- tcgen05 kind::i8 -- only for m <= 128, k <= 64, n <= 64),
    1 CUDA cores only, 2 tensor cores wherever the shape allows.
-   The environment variable MPZMM_CONTRACT sets the initial value. */
+   The environment variable MPZMM_CONTRACT sets the initial value.
+   MPZMM_OPT_CHUNK_LIMBS sets the input limbs per chunk of a pipelined
+   one-shot batch (mpzmm_matmul_batch): 0 (default) chooses an eighth of
+   the batch, at least 2^24 limbs; a batch no larger than one chunk runs
+   unchunked. */
 #define MPZMM_OPT_CONTRACT 1
+#define MPZMM_OPT_CHUNK_LIMBS 2
 MPZMM_API int mpzmm_set_option(int option, int value);
 MPZMM_API int mpzmm_get_option(int option);
+
+/* Pinned host memory.  Copies whose host side lies wholly inside memory
+   from mpzmm_host_alloc, or inside a range registered with
+   mpzmm_host_register (cudaHostRegister), go straight between that memory
+   and the device: no staging copy, and the DMA runs at full link speed.
+   Other host memory is staged through the library's pinned buffers. */
+MPZMM_API int mpzmm_host_alloc(size_t bytes, void **out);
+MPZMM_API int mpzmm_host_free(void *p);
+MPZMM_API int mpzmm_host_register(void *p, size_t bytes);
+MPZMM_API int mpzmm_host_unregister(void *p);
+
+/* Statistics of the last one-shot batch (mpzmm_matmul_batch, mpzmm_matmul,
+   mpz_rmatrix_mult_fft), summed over its chunks (any pointer may be NULL):
+   host nanoseconds ns4[0] planning, [1] input copies (staging and
+   queueing), [2] kernel and output copy queueing, [3] waiting and writing
+   results; the chunk count; bytes4[0] host->device and [1] device->host
+   bytes, [2] and [3] the parts of those that moved straight between the
+   caller's pinned memory and the device. */
+MPZMM_API int mpzmm_batch_stats(int64_t *ns4, int64_t *chunks, int64_t *bytes4);
 
 /* Autotuner: times the contraction of a representative product per size
    class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
@@ -151,7 +175,14 @@ typedef struct mpzmm_product {
 } mpzmm_product;
 
 /* Many independent products of uneven shapes and sizes in one pass: one
-   launch per pipeline stage for the whole batch.  Synchronous. */
+   launch per pipeline stage and size class for the batch, or, for a batch
+   larger than one chunk (MPZMM_OPT_CHUNK_LIMBS), per chunk of whole
+   products, with the chunks pipelined so that copies in both directions
+   overlap the kernels.  Operand arrays in pinned memory (mpzmm_host_alloc /
+   mpzmm_host_register) are copied without staging, short gaps between
+   entries included; an output array takes the device's words directly when
+   its entries are evenly spaced with capacity at least
+   mpzmm_output_limbs(k, exact operand bit lengths).  Synchronous. */
 MPZMM_API int mpzmm_matmul_batch(int count, const mpzmm_product *products, void *stream);
 
 /* ---- device-resident plans (build once, run many times) ---- */

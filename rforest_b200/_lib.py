@@ -20,6 +20,7 @@ MPZMM_ERR_TIMEOUT = 7
 MPZMM_ERR_BUSY = 8
 
 MPZMM_OPT_CONTRACT = 1
+MPZMM_OPT_CHUNK_LIMBS = 2
 CONTRACT_AUTO, CONTRACT_CUDA_CORES, CONTRACT_TENSOR_CORES = 0, 1, 2
 
 u64p = C.POINTER(C.c_uint64)
@@ -99,6 +100,11 @@ def lib():
         "mpzmm_server_stats": (C.c_int, [vp, i64p, i64p, i64p]),
         "mpzmm_server_destroy": (None, [vp]),
         "mpzmm_server_phase_ns": (C.c_int, [vp, i64p]),
+        "mpzmm_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
+        "mpzmm_host_free": (C.c_int, [vp]),
+        "mpzmm_host_register": (C.c_int, [vp, C.c_size_t]),
+        "mpzmm_host_unregister": (C.c_int, [vp]),
+        "mpzmm_batch_stats": (C.c_int, [i64p, i64p, i64p]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

@@ -53,6 +53,57 @@ def autotune(stream=None):
     return out
 
 
+def set_chunk_limbs(limbs: int) -> None:
+    """Input limbs per chunk of a pipelined one-shot batch (0 = automatic)."""
+    _lib.check(_lib.lib().mpzmm_set_option(_lib.MPZMM_OPT_CHUNK_LIMBS, int(limbs)))
+
+
+def chunk_limbs() -> int:
+    return int(_lib.lib().mpzmm_get_option(_lib.MPZMM_OPT_CHUNK_LIMBS))
+
+
+def batch_stats():
+    """Last one-shot batch: host time in ms (plan, input copies, launch
+    queueing, wait + results), chunk count, and bytes copied each way (with
+    the parts that moved straight from / to pinned caller memory)."""
+    ns = (C.c_int64 * 4)()
+    nb = (C.c_int64 * 4)()
+    chunks = C.c_int64()
+    _lib.check(_lib.lib().mpzmm_batch_stats(ns, C.byref(chunks), nb))
+    return {"plan_ms": ns[0] / 1e6, "inputs_ms": ns[1] / 1e6, "launch_ms": ns[2] / 1e6,
+            "finish_ms": ns[3] / 1e6, "chunks": chunks.value,
+            "h2d_bytes": nb[0], "d2h_bytes": nb[1],
+            "h2d_direct_bytes": nb[2], "d2h_direct_bytes": nb[3]}
+
+
+class HostArena:
+    """Pinned host memory from the library (mpzmm_host_alloc).  Transfers
+    whose host side lies inside it go straight to and from the device."""
+
+    def __init__(self, nbytes: int):
+        self.nbytes = max(int(nbytes), 8)
+        p = C.c_void_p()
+        _lib.check(_lib.lib().mpzmm_host_alloc(self.nbytes, C.byref(p)))
+        self.ptr = p.value
+        self.used = 0
+
+    def take(self, count: int, dtype) -> np.ndarray:
+        """Next ``count`` elements of ``dtype`` (8-byte aligned) as a numpy view."""
+        dt = np.dtype(dtype)
+        off = (self.used + 7) & ~7
+        nb = max(int(count), 1) * dt.itemsize
+        if off + nb > self.nbytes:
+            raise MemoryError("host arena exhausted")
+        self.used = off + nb
+        buf = (C.c_char * nb).from_address(self.ptr + off)
+        return np.frombuffer(buf, dtype=dt, count=max(int(count), 1))
+
+    def close(self) -> None:
+        if self.ptr:
+            _lib.check(_lib.lib().mpzmm_host_free(C.c_void_p(self.ptr)))
+            self.ptr = None
+
+
 def contract_mode() -> int:
     return int(_lib.lib().mpzmm_get_option(_lib.MPZMM_OPT_CONTRACT))
 
@@ -75,12 +126,19 @@ def output_limbs(k: int, a_bits: int, b_bits: int) -> int:
 class _Holder:
     """Keeps the numpy arrays behind one mpzmm_product alive."""
 
-    def __init__(self, m: int, k: int, n: int, A: Packed, B: Packed):
+    def __init__(self, m: int, k: int, n: int, A: Packed, B: Packed, bufs=None):
+        """``bufs``: optional (a_limbs, b_limbs, c_limbs) arrays to use (for
+        example views into a pinned arena); the inputs are copied into them."""
         if len(A) != m * k or len(B) != k * n:
             raise ValueError("entry counts do not match the dimensions")
         self.m, self.k, self.n = m, k, n
-        self.al = np.ascontiguousarray(A.limbs, dtype=np.uint64)
-        self.bl = np.ascontiguousarray(B.limbs, dtype=np.uint64)
+        if bufs is not None:
+            self.al, self.bl = bufs[0], bufs[1]
+            np.copyto(self.al[:A.limbs.size], A.limbs)
+            np.copyto(self.bl[:B.limbs.size], B.limbs)
+        else:
+            self.al = np.ascontiguousarray(A.limbs, dtype=np.uint64)
+            self.bl = np.ascontiguousarray(B.limbs, dtype=np.uint64)
         if self.al.size == 0:
             self.al = np.zeros(1, np.uint64)
         if self.bl.size == 0:
@@ -89,10 +147,13 @@ class _Holder:
         self.bo = np.ascontiguousarray(B.offs, dtype=np.int64)
         self.asz = np.ascontiguousarray(A.sizes, dtype=np.int32)
         self.bsz = np.ascontiguousarray(B.sizes, dtype=np.int32)
-        cap = output_limbs(k, 64 * A.max_limbs(), 64 * B.max_limbs())
+        cap = self.out_cap(k, A, B)
         self.caps = np.full(m * n, cap, dtype=np.int64)
         self.co = np.arange(m * n, dtype=np.int64) * cap
-        self.cl = np.zeros(max(m * n * cap, 1), dtype=np.uint64)
+        if bufs is not None:
+            self.cl = bufs[2]
+        else:
+            self.cl = np.zeros(max(m * n * cap, 1), dtype=np.uint64)
         self.csz = np.zeros(m * n, dtype=np.int32)
         self.struct = _lib.Product(
             m, k, n,
@@ -100,6 +161,12 @@ class _Holder:
             _ptr(self.bl, _lib.u64p), _ptr(self.bo, _lib.i64p), _ptr(self.bsz, _lib.i32p),
             _ptr(self.cl, _lib.u64p), _ptr(self.co, _lib.i64p), _ptr(self.caps, _lib.i64p),
             _ptr(self.csz, _lib.i32p))
+
+    @staticmethod
+    def out_cap(k: int, A: Packed, B: Packed) -> int:
+        """The library's own bound for the product (exact operand bit
+        lengths), so results fill the output array back to back."""
+        return output_limbs(k, A.max_bits(), B.max_bits())
 
     def result(self) -> Packed:
         return Packed(self.cl, self.co, self.csz)
@@ -123,14 +190,42 @@ class Batch:
     host->device copy of the inputs, all kernels, device->host copy of the
     results into the host output arrays."""
 
-    def __init__(self, products: Sequence[ProductIn]):
-        self.holders = [_Holder(*p) for p in products]
+    def __init__(self, products: Sequence[ProductIn], pinned: bool = False):
+        """With ``pinned`` the inputs are copied (once, here) into one pinned
+        arena from the library and the outputs live there too, so every
+        ``run`` moves them straight between that memory and the device.  The
+        results of a pinned batch are views into the arena: valid until
+        ``close``."""
+        self.arena = None
+        bufs = [None] * len(products)
+        if pinned:
+            caps = [_Holder.out_cap(p[1], p[3], p[4]) for p in products]
+            nbytes = 64
+            for (m, k, n, A, B), cap in zip(products, caps):
+                nbytes += 8 * (max(A.limbs.size, 1) + max(B.limbs.size, 1)
+                               + max(m * n * cap, 1)) + 24
+            self.arena = HostArena(nbytes)
+            # all inputs back to back (one copy run for the batch), then all
+            # outputs
+            ins = [(self.arena.take(A.limbs.size, np.uint64),
+                    self.arena.take(B.limbs.size, np.uint64)) for (m, k, n, A, B) in products]
+            outs = [self.arena.take(max(p[0] * p[2] * cap, 1), np.uint64)
+                    for p, cap in zip(products, caps)]
+            bufs = [(a, b, c) for (a, b), c in zip(ins, outs)]
+        self.holders = [_Holder(*p, bufs=bb) for p, bb in zip(products, bufs)]
         self.arr = (_lib.Product * len(self.holders))(*[h.struct for h in self.holders])
 
     def run(self, stream=None) -> List[Packed]:
         _lib.check(_lib.lib().mpzmm_matmul_batch(len(self.holders), self.arr,
                                                  _stream_arg(stream)))
         return [h.result() for h in self.holders]
+
+    def close(self) -> None:
+        self.holders = []
+        self.arr = None
+        if self.arena is not None:
+            self.arena.close()
+            self.arena = None
 
 
 def matmul_batch(products: Sequence[ProductIn], stream=None) -> List[Packed]:

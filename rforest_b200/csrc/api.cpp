@@ -52,12 +52,7 @@ int run_once(std::vector<ProductSpec> specs, void* stream) {
   int st = ensure_setup(-1);
   if (st) return st;
   std::lock_guard<std::mutex> lk(workspace_mutex());
-  Plan plan;
-  if ((st = plan.build(std::move(specs), context().ws))) return st;
-  cudaStream_t s = pick_stream(stream);
-  if ((st = plan.upload(s))) return st;
-  if ((st = plan.execute(s))) return st;
-  return plan.download(s);
+  return run_batch(std::move(specs), pick_stream(stream));
 }
 
 // r x d by d x d over mpz_t arrays (src/lib/hwmpz.c:65-130)
@@ -96,6 +91,12 @@ int mpzmm_set_option(int option, int value) {
   if (option == MPZMM_OPT_CONTRACT) {
     if (value < 0 || value > 2) return set_error(kErrArg, "contract mode must be 0, 1 or 2");
     context().contract_mode = value;
+    return kOk;
+  }
+  if (option == MPZMM_OPT_CHUNK_LIMBS) {
+    if (value < 0) return set_error(kErrArg, "chunk size must be >= 0");
+    std::lock_guard<std::mutex> lk(workspace_mutex());
+    context().chunk_limbs = value;
     return kOk;
   }
   return set_error(kErrArg, "unknown option");
@@ -172,7 +173,23 @@ int mpzmm_autotune(void* stream, float* ms_out) {
 
 int mpzmm_get_option(int option) {
   if (option == MPZMM_OPT_CONTRACT) return context().contract_mode;
+  if (option == MPZMM_OPT_CHUNK_LIMBS) return (int)context().chunk_limbs;
   return -1;
+}
+
+int mpzmm_host_alloc(size_t bytes, void** out) { return host_alloc(bytes, out); }
+int mpzmm_host_free(void* p) { return host_free(p); }
+int mpzmm_host_register(void* p, size_t bytes) { return host_register(p, bytes); }
+int mpzmm_host_unregister(void* p) { return host_unregister(p); }
+
+int mpzmm_batch_stats(int64_t* ns4, int64_t* chunks, int64_t* bytes4) {
+  std::lock_guard<std::mutex> lk(workspace_mutex());
+  for (int i = 0; i < 4; ++i) {
+    if (ns4) ns4[i] = context().batch_ns[i];
+    if (bytes4) bytes4[i] = context().batch_bytes[i];
+  }
+  if (chunks) *chunks = context().batch_chunks;
+  return kOk;
 }
 
 const char* mpzmm_last_error(void) { return last_error(); }

@@ -2,9 +2,13 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <utility>
@@ -21,6 +25,10 @@ std::mutex g_ctx_mu;
 
 int cuda_fail(cudaError_t e, const char* what) {
   return set_error(kErrCuda, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  return e == cudaSuccess ? kOk : cuda_fail(e, what);
 }
 
 #define CU(call, what)                          \
@@ -89,6 +97,92 @@ void parallel_chunks(size_t n, size_t bytes, const std::function<void(size_t, si
   for (auto& t : th) t.join();
 }
 
+// ---- pinned host memory known to the library ----
+namespace {
+struct HostRange {
+  size_t bytes;
+  bool owned;  // allocated here (else registered)
+};
+std::mutex g_host_mu;
+std::map<uintptr_t, HostRange> g_host;
+}  // namespace
+
+std::vector<std::pair<uintptr_t, size_t>> pinned_ranges() {
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  std::vector<std::pair<uintptr_t, size_t>> v;
+  v.reserve(g_host.size());
+  for (const auto& kv : g_host) v.emplace_back(kv.first, kv.second.bytes);
+  return v;  // sorted by start
+}
+
+bool in_ranges(const std::vector<std::pair<uintptr_t, size_t>>& v, const void* p, size_t bytes) {
+  if (!p || !bytes || v.empty()) return false;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  auto it = std::upper_bound(v.begin(), v.end(), std::make_pair(a, ~(size_t)0));
+  if (it == v.begin()) return false;
+  --it;
+  return a - it->first <= it->second && bytes <= it->second - (a - it->first);
+}
+
+uintptr_t range_end(const std::vector<std::pair<uintptr_t, size_t>>& v, const void* p,
+                    size_t bytes) {
+  if (!in_ranges(v, p, bytes)) return 0;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  auto it = std::upper_bound(v.begin(), v.end(), std::make_pair(a, ~(size_t)0));
+  --it;
+  return it->first + it->second;
+}
+
+bool host_range_pinned(const void* p, size_t bytes) { return in_ranges(pinned_ranges(), p, bytes); }
+
+int host_alloc(size_t bytes, void** out) {
+  if (!out) return set_error(kErrArg, "null output pointer");
+  *out = nullptr;
+  if (!bytes) return set_error(kErrArg, "zero-byte host allocation");
+  int st = ensure_setup(-1);
+  if (st) return st;
+  void* p = nullptr;
+  cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess)
+    return set_error(kErrNoMem, std::string("cudaHostAlloc of ") + std::to_string(bytes) +
+                                    " bytes: " + cudaGetErrorString(e));
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  g_host[reinterpret_cast<uintptr_t>(p)] = HostRange{bytes, true};
+  *out = p;
+  return kOk;
+}
+
+int host_free(void* p) {
+  if (!p) return kOk;
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  auto it = g_host.find(reinterpret_cast<uintptr_t>(p));
+  if (it == g_host.end() || !it->second.owned)
+    return set_error(kErrArg, "pointer was not allocated by mpzmm_host_alloc");
+  g_host.erase(it);
+  CU(cudaFreeHost(p), "cudaFreeHost");
+  return kOk;
+}
+
+int host_register(void* p, size_t bytes) {
+  if (!p || !bytes) return set_error(kErrArg, "null or empty host range");
+  int st = ensure_setup(-1);
+  if (st) return st;
+  CU(cudaHostRegister(p, bytes, cudaHostRegisterPortable), "cudaHostRegister");
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  g_host[reinterpret_cast<uintptr_t>(p)] = HostRange{bytes, false};
+  return kOk;
+}
+
+int host_unregister(void* p) {
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  auto it = g_host.find(reinterpret_cast<uintptr_t>(p));
+  if (it == g_host.end() || it->second.owned)
+    return set_error(kErrArg, "pointer was not registered by mpzmm_host_register");
+  g_host.erase(it);
+  CU(cudaHostUnregister(p), "cudaHostUnregister");
+  return kOk;
+}
+
 int ensure_setup(int device) {
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   if (g_ctx.ready) {
@@ -143,6 +237,19 @@ void teardown() {
   cudaFree(g_ctx.d_twi);
   {
     std::lock_guard<std::mutex> wl(workspace_mutex());
+    for (cudaStream_t s : g_ctx.pipe_st) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+    for (cudaStream_t s : {g_ctx.pipe_in, g_ctx.pipe_out})
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    for (size_t i = 1; i < g_ctx.pipe_ws.size(); ++i) delete g_ctx.pipe_ws[i];
+    if (g_ctx.pipe_ev) cudaEventDestroy(g_ctx.pipe_ev);
+    for (auto* v : {&g_ctx.pipe_ev_in, &g_ctx.pipe_ev_exec, &g_ctx.pipe_ev_out})
+      for (cudaEvent_t e : *v) cudaEventDestroy(e);
     delete g_ctx.ws;
   }
   cudaStreamDestroy(g_ctx.stream);
@@ -156,7 +263,7 @@ Plan::~Plan() {
 }
 
 int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
-                       size_t desc_bytes) {
+                       size_t desc_bytes, size_t stage_limbs, size_t stage_out_words) {
   // device: check the total growth against free memory first
   size_t grow = 0;
   if (limbs > cap_limbs) grow += limbs * 8;
@@ -241,10 +348,17 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
     }
     device_bytes += (int64_t)sizeof(int);
   }
-  if ((st = grow_host(&h_limbs, hcap_limbs, limbs, 8))) return st;
-  if ((st = grow_host(&h_out, hcap_out, out_words, 4))) return st;
+  if ((st = grow_host(&h_limbs, hcap_limbs, stage_limbs, 8))) return st;
+  if ((st = grow_host(&h_out, hcap_out, stage_out_words, 4))) return st;
   if ((st = grow_host(&h_sizes, hcap_sizes, sizes, 4))) return st;
   if ((st = grow_host(&h_desc, hcap_desc, desc_bytes, 1))) return st;
+  if (!h_status) {
+    cudaError_t e = cudaMallocHost((void**)&h_status, sizeof(int));
+    if (e != cudaSuccess) {
+      h_status = nullptr;
+      return set_error(kErrNoMem, std::string("cudaMallocHost(status): ") + cudaGetErrorString(e));
+    }
+  }
   return kOk;
 }
 
@@ -272,10 +386,12 @@ void Workspace::release() {
   cudaFreeHost(h_out);
   cudaFreeHost(h_sizes);
   cudaFreeHost(h_desc);
+  cudaFreeHost(h_status);
   h_limbs = nullptr;
   h_out = nullptr;
   h_sizes = nullptr;
   h_desc = nullptr;
+  h_status = nullptr;
   hcap_limbs = hcap_out = hcap_sizes = hcap_desc = 0;
 }
 
@@ -312,6 +428,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   std::map<int, int64_t> rec_min_r;
 
   uint64_t out_entry = 0;
+  const uint64_t* host_end = nullptr;  // end of the previous entry's host limbs
+  uintptr_t run_pinned_end = 0;        // end of the pinned range of the current run (0: none)
+  const auto pinned = pinned_ranges();
+  in_runs_.clear();
   for (size_t t = 0; t < prods_.size(); ++t) {
     ProductSpec& ps = prods_[t];
     const int m = ps.m, k = ps.k, n = ps.n;
@@ -342,7 +462,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     out_entry += ps.c.size();
     if (prm.P == 0 || m == 0 || n == 0) {
       zero_prod_[t] = 1;
-      for (size_t e = 0; e < ps.c.size(); ++e) out_word_off_.push_back(-1);
+      for (size_t e = 0; e < ps.c.size(); ++e) {
+        out_word_off_.push_back(-1);
+        out_limbs_.push_back(0);
+      }
       continue;
     }
     const int P = prm.P, lgN = prm.lgN, r = prm.r;
@@ -370,6 +493,34 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       for (size_t e = 0; e < ents.size(); ++e) {
         FwdDesc fd;
         const int64_t nl = ents[e].size < 0 ? -(int64_t)ents[e].size : ents[e].size;
+        if (nl) {
+          // Copy runs: an entry continues the current run when it follows
+          // the previous one in host memory -- directly, or, inside one
+          // pinned range, after a short gap (the run then copies the gap
+          // too and the device layout mirrors it).  A new run starts at the
+          // same address modulo 256 bytes as its host limbs, so the copy
+          // engine moves aligned bursts.
+          const uint64_t* d = ents[e].d;
+          const uintptr_t dend = reinterpret_cast<uintptr_t>(d + nl);
+          bool join = false;
+          if (host_end && (!run_pinned_end || dend <= run_pinned_end)) {
+            if (d == host_end) {
+              join = true;
+            } else if (run_pinned_end && d > host_end && d - host_end <= kRunGapLimbs) {
+              n_limbs_ += (uint64_t)(d - host_end);
+              join = true;
+            }
+          }
+          if (join) {
+            in_runs_.back().n = n_limbs_ + (uint64_t)nl - in_runs_.back().dev;
+          } else {
+            run_pinned_end = range_end(pinned, d, (size_t)nl * 8);
+            const uint64_t want = (reinterpret_cast<uintptr_t>(d) >> 3) & 31;
+            n_limbs_ += (want - n_limbs_) & 31;
+            in_runs_.push_back(Run{d, n_limbs_, (uint64_t)nl, 0, run_pinned_end != 0, 1, 0});
+          }
+          host_end = d + nl;
+        }
         fd.limb_off = n_limbs_;
         n_limbs_ += (uint64_t)nl;
         fd.res_off = base + e * poly;
@@ -413,6 +564,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       id.out_word = n_out_words_;
       id.out_words = (uint32_t)(2 * prm.out_limbs);
       out_word_off_.push_back((int64_t)n_out_words_);
+      out_limbs_.push_back((int32_t)prm.out_limbs);
       n_out_words_ += id.out_words;
       id.r = (uint32_t)r;
       id.ncoef = (uint32_t)(ncoef_c < N ? ncoef_c : N);
@@ -509,8 +661,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   off_idx_ = align16(off_tc_ + tc_items_.size() * sizeof(ContractItem));
   off_cta_ = align16(off_idx_ + idx_all_.size() * sizeof(uint32_t));
   desc_bytes_ = align16(off_cta_ + cta_items_.size() * sizeof(CtaItem));
+  plan_transfers();
   ws_ = ws ? ws : &own_;
-  int st = ws_->reserve(n_limbs_, n_res_, n_out_words_, outs_.size(), desc_bytes_);
+  int st = ws_->reserve(n_limbs_, n_res_, n_out_words_, outs_.size(), desc_bytes_, stage_limbs_,
+                        stage_out_words_);
   if (st) return st;
   uint8_t* hd = ws_->h_desc;
   if (!fwd_.empty()) std::memcpy(hd + off_fwd_, fwd_.data(), fwd_.size() * sizeof(FwdDesc));
@@ -538,42 +692,136 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   return kOk;
 }
 
-int Plan::upload(cudaStream_t st) {
-  if (!built_) return set_error(kErrState, "plan not built");
-  // flat list of (source, destination, limbs) to gather in parallel
-  struct Copy {
-    const uint64_t* src;
-    uint64_t dst;
-    int64_t n;
-  };
-  std::vector<Copy> copies;
-  copies.reserve(fwd_.size());
-  size_t fi = 0;
-  for (size_t t = 0; t < prods_.size(); ++t) {
-    if (zero_prod_[t]) continue;
-    const ProductSpec& ps = prods_[t];
-    for (int side = 0; side < 2; ++side) {
-      const auto& ents = side ? ps.b : ps.a;
-      for (const auto& e : ents) {
-        const FwdDesc& fd = fwd_[fi++];
-        const int64_t nl = e.size < 0 ? -(int64_t)e.size : e.size;
-        if (nl != (fd.size < 0 ? -(int64_t)fd.size : fd.size) || (e.size < 0) != (fd.size < 0))
-          return set_error(kErrArg, "inputs changed size or sign since the plan was built");
-        if (nl) copies.push_back(Copy{e.d, fd.limb_off, nl});
-      }
+void Plan::plan_transfers() {
+  out_runs_.clear();
+  stage_limbs_ = stage_out_words_ = direct_in_limbs_ = direct_out_words_ = 0;
+  // inputs: runs were formed while the limb offsets were assigned
+  for (Run& r : in_runs_) {
+    if (r.direct) {
+      direct_in_limbs_ += r.n;
+    } else {
+      stage_limbs_ += (r.dev - stage_limbs_) & 31;  // same 256-byte phase as the device side
+      r.stage = stage_limbs_;
+      stage_limbs_ += r.n;
     }
   }
-  uint64_t* hl = ws_->h_limbs;
-  parallel_chunks(copies.size(), (size_t)n_limbs_ * 8, [&](size_t lo, size_t hi) {
-    for (size_t i = lo; i < hi; ++i)
-      std::memcpy(hl + copies[i].dst, copies[i].src, (size_t)copies[i].n * 8);
-  });
+  // outputs, per product: packed destinations in pinned memory, entries at
+  // a constant stride with room for every word the device writes, take the
+  // device's words straight (one copy, strided when the stride exceeds the
+  // device's); everything else (mpz destinations included) is staged
+  const auto pinned = pinned_ranges();
+  out_stage_.assign(outs_.size(), -1);
+  size_t e0 = 0;
+  for (size_t t = 0; t < prods_.size(); ++t) {
+    const size_t cnt = prods_[t].c.size();
+    const size_t first = e0;
+    e0 += cnt;
+    if (!cnt || zero_prod_[t]) continue;
+    const int64_t lim = out_limbs_[first];
+    const uint64_t width = 2 * (uint64_t)lim;  // words per entry on the device
+    const uint64_t dev = (uint64_t)out_word_off_[first];
+    bool can = true;
+    int64_t stride = 0;  // limbs between consecutive destinations
+    for (size_t e = first; e < first + cnt && can; ++e) {
+      const OutRef& o = outs_[e];
+      can = o.d && !o.mpz && o.cap >= lim;
+      if (can && e > first) {
+        const int64_t d = o.d - outs_[e - 1].d;
+        if (e == first + 1) stride = d;
+        can = d == stride && d >= lim;
+      }
+    }
+    if (cnt == 1) stride = lim;
+    if (can) {
+      const size_t span = (size_t)((cnt - 1) * (uint64_t)stride + (uint64_t)lim) * 8;
+      can = in_ranges(pinned, outs_[first].d, span);
+    }
+    if (can && stride == lim) {
+      // back to back: a plain copy, merged with the previous product's when
+      // both sides continue it
+      if (!out_runs_.empty()) {
+        Run& b = out_runs_.back();
+        if (b.direct && b.rows == 1 && b.dev + b.n == dev &&
+            static_cast<const uint32_t*>(b.host) + b.n ==
+                reinterpret_cast<const uint32_t*>(outs_[first].d)) {
+          b.n += width * cnt;
+          direct_out_words_ += width * cnt;
+          continue;
+        }
+      }
+      out_runs_.push_back(Run{outs_[first].d, dev, width * cnt, 0, true, 1, 0});
+      direct_out_words_ += width * cnt;
+    } else if (can) {
+      out_runs_.push_back(Run{outs_[first].d, dev, width, 0, true, (uint64_t)cnt,
+                              2 * (uint64_t)stride});
+      direct_out_words_ += width * cnt;
+    } else {
+      for (size_t e = first; e < first + cnt; ++e)
+        out_stage_[e] = (int64_t)(stage_out_words_ + (uint64_t)out_word_off_[e] - dev);
+      if (!out_runs_.empty()) {
+        Run& b = out_runs_.back();
+        if (!b.direct && b.dev + b.n == dev && b.stage + b.n == stage_out_words_) {
+          b.n += width * cnt;
+          stage_out_words_ += width * cnt;
+          continue;
+        }
+      }
+      out_runs_.push_back(Run{nullptr, dev, width * cnt, stage_out_words_, false, 1, 0});
+      stage_out_words_ += width * cnt;
+    }
+  }
+}
+
+int Plan::upload(cudaStream_t st) {
+  if (!built_) return set_error(kErrState, "plan not built");
   if (desc_bytes_)
     CU(cudaMemcpyAsync(ws_->d_desc, ws_->h_desc, desc_bytes_, cudaMemcpyHostToDevice, st),
        "H2D descriptors");
   CU(cudaMemsetAsync(ws_->d_status, 0, sizeof(int), st), "clear status");
-  if (n_limbs_)
-    CU(cudaMemcpyAsync(ws_->d_limbs, hl, n_limbs_ * 8, cudaMemcpyHostToDevice, st), "H2D limbs");
+  // straight copies first, so the DMA runs while the staged runs are gathered
+  for (const Run& r : in_runs_)
+    if (r.direct)
+      CU(cudaMemcpyAsync(ws_->d_limbs + r.dev, r.host, r.n * 8, cudaMemcpyHostToDevice, st),
+         "H2D limbs");
+  if (!stage_limbs_) return kOk;
+  // staged runs: gathered in pieces of at most 4 MB across host threads
+  struct Piece {
+    const uint64_t* src;
+    uint64_t stage, n;
+  };
+  constexpr uint64_t kPiece = (4ull << 20) / 8;
+  std::vector<Piece> pieces;
+  for (const Run& r : in_runs_) {
+    if (r.direct) continue;
+    for (uint64_t o = 0; o < r.n; o += kPiece)
+      pieces.push_back(Piece{static_cast<const uint64_t*>(r.host) + o, r.stage + o,
+                             r.n - o < kPiece ? r.n - o : kPiece});
+  }
+  uint64_t* hl = ws_->h_limbs;
+  parallel_chunks(pieces.size(), (size_t)stage_limbs_ * 8, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i)
+      std::memcpy(hl + pieces[i].stage, pieces[i].src, (size_t)pieces[i].n * 8);
+  });
+  // consecutive staged runs go as one copy: their alignment gaps are the
+  // same on both sides (staging mirrors the device's 256-byte phase), and
+  // the gap words are padding nobody reads
+  size_t i = 0;
+  while (i < in_runs_.size()) {
+    if (in_runs_[i].direct) {
+      ++i;
+      continue;
+    }
+    uint64_t dev = in_runs_[i].dev, stg = in_runs_[i].stage, n = in_runs_[i].n;
+    size_t j = i + 1;
+    while (j < in_runs_.size() && !in_runs_[j].direct && in_runs_[j].dev >= dev + n &&
+           in_runs_[j].dev - (dev + n) == in_runs_[j].stage - (stg + n)) {
+      n = in_runs_[j].dev + in_runs_[j].n - dev;
+      ++j;
+    }
+    CU(cudaMemcpyAsync(ws_->d_limbs + dev, hl + stg, n * 8, cudaMemcpyHostToDevice, st),
+       "H2D limbs");
+    i = j;
+  }
   return kOk;
 }
 
@@ -670,22 +918,37 @@ void Plan::stage_launches(int64_t out[kStages]) const {
   out[3] = (int64_t)rec_groups_.size();
 }
 
-int Plan::download(cudaStream_t st) {
+int Plan::download_enqueue(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
-  int32_t* hs = ws_->h_sizes;
-  uint32_t* ho = ws_->h_out;
   if (!outs_.empty() && !inv_.empty())
-    CU(cudaMemcpyAsync(hs, ws_->d_sizes, outs_.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                       st),
+    CU(cudaMemcpyAsync(ws_->h_sizes, ws_->d_sizes, outs_.size() * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st),
        "D2H sizes");
-  if (n_out_words_)
-    CU(cudaMemcpyAsync(ho, ws_->d_out, n_out_words_ * 4, cudaMemcpyDeviceToHost, st), "D2H words");
-  int kstatus = 0;
-  CU(cudaMemcpyAsync(&kstatus, ws_->d_status, sizeof(int), cudaMemcpyDeviceToHost, st),
+  for (const Run& r : out_runs_) {
+    void* dst = r.direct ? const_cast<void*>(r.host) : (void*)(ws_->h_out + r.stage);
+    if (r.rows > 1)
+      CU(cudaMemcpy2DAsync(dst, r.pitch * 4, ws_->d_out + r.dev, r.n * 4, r.n * 4, r.rows,
+                           cudaMemcpyDeviceToHost, st),
+         "D2H words (strided)");
+    else
+      CU(cudaMemcpyAsync(dst, ws_->d_out + r.dev, r.n * 4, cudaMemcpyDeviceToHost, st),
+         "D2H words");
+  }
+  CU(cudaMemcpyAsync(ws_->h_status, ws_->d_status, sizeof(int), cudaMemcpyDeviceToHost, st),
      "D2H status");
-  CU(cudaStreamSynchronize(st), "kernel execution");
-  if (kstatus)
+  return kOk;
+}
+
+int Plan::download_finish(cudaStream_t st, cudaEvent_t done) {
+  if (!built_) return set_error(kErrState, "plan not built");
+  if (done)
+    CU(cudaEventSynchronize(done), "kernel execution");
+  else
+    CU(cudaStreamSynchronize(st), "kernel execution");
+  if (*ws_->h_status)
     return set_error(kErrTimeout, "a tensor-core contraction wait timed out; results invalid");
+  const int32_t* hs = ws_->h_sizes;
+  const uint32_t* ho = ws_->h_out;
   // capacity check first (serial, cheap), then the copies in parallel
   int status = kOk;
   std::vector<uint8_t> ok(outs_.size(), 1);
@@ -704,24 +967,246 @@ int Plan::download(cudaStream_t st) {
       if (o.size) *o.size = 0;
     }
   }
-  parallel_chunks(outs_.size(), (size_t)n_out_words_ * 4, [&](size_t lo, size_t hi) {
+  parallel_chunks(outs_.size(), (size_t)stage_out_words_ * 4, [&](size_t lo, size_t hi) {
     for (size_t e = lo; e < hi; ++e) {
       if (!ok[e]) continue;
       const OutRef& o = outs_[e];
-      const int64_t woff = out_word_off_[e];
-      const int32_t sz = woff < 0 ? 0 : hs[e];
+      const int32_t sz = out_word_off_[e] < 0 ? 0 : hs[e];
       const int64_t nl = sz < 0 ? -(int64_t)sz : sz;
-      const uint64_t* src = woff < 0 ? nullptr : reinterpret_cast<const uint64_t*>(ho + woff);
+      const int64_t so = out_stage_[e];
+      const uint64_t* src = so < 0 ? nullptr : reinterpret_cast<const uint64_t*>(ho + so);
       if (o.mpz) {
         __mpz_struct* z = static_cast<__mpz_struct*>(o.mpz);
         if (nl) std::memcpy(z->_mp_d, src, (size_t)nl * 8);
         z->_mp_size = sz;
       } else {
-        if (nl) std::memcpy(o.d, src, (size_t)nl * 8);
+        if (nl && src) std::memcpy(o.d, src, (size_t)nl * 8);  // else already in place
         if (o.size) *o.size = sz;
       }
     }
   });
+  return status;
+}
+
+int Plan::download(cudaStream_t st) {
+  int s = download_enqueue(st);
+  return s ? s : download_finish(st);
+}
+
+// ---- one-shot batches ----
+namespace {
+int64_t now_ns() {
+  return std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+uint64_t input_limbs(const ProductSpec& ps) {
+  uint64_t n = 0;
+  for (const auto& e : ps.a) n += e.size < 0 ? (uint64_t)(-(int64_t)e.size) : (uint64_t)e.size;
+  for (const auto& e : ps.b) n += e.size < 0 ? (uint64_t)(-(int64_t)e.size) : (uint64_t)e.size;
+  return n;
+}
+
+int ensure_pipeline(Context& ctx) {
+  while ((int)ctx.pipe_ws.size() < kPipeDepth)
+    ctx.pipe_ws.push_back(ctx.pipe_ws.empty() ? ctx.ws : new Workspace);
+  while ((int)ctx.pipe_st.size() < kPipeDepth) {
+    cudaStream_t s = nullptr;
+    CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    ctx.pipe_st.push_back(s);
+  }
+  for (cudaStream_t* s : {&ctx.pipe_in, &ctx.pipe_out})
+    if (!*s) CU(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!ctx.pipe_ev)
+    CU(cudaEventCreateWithFlags(&ctx.pipe_ev, cudaEventDisableTiming), "cudaEventCreate");
+  for (auto* v : {&ctx.pipe_ev_in, &ctx.pipe_ev_exec, &ctx.pipe_ev_out})
+    while ((int)v->size() < kPipeDepth) {
+      cudaEvent_t e = nullptr;
+      CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+      v->push_back(e);
+    }
+  return kOk;
+}
+}  // namespace
+
+int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
+  Context& ctx = context();
+  for (auto& v : ctx.batch_ns) v = 0;
+  for (auto& v : ctx.batch_bytes) v = 0;
+  auto count_bytes = [&ctx](const Plan& p) {
+    ctx.batch_bytes[0] += (int64_t)p.upload_bytes();
+    ctx.batch_bytes[1] += (int64_t)p.download_bytes();
+    ctx.batch_bytes[2] += (int64_t)p.direct_in_bytes();
+    ctx.batch_bytes[3] += (int64_t)p.direct_out_bytes();
+  };
+  uint64_t total = 0;
+  std::vector<uint64_t> limbs(specs.size());
+  for (size_t t = 0; t < specs.size(); ++t) total += (limbs[t] = input_limbs(specs[t]));
+  // automatic chunks: an eighth of the batch, at least 16 Mi limbs (128 MB)
+  uint64_t chunk = ctx.chunk_limbs > 0 ? (uint64_t)ctx.chunk_limbs : total / 8;
+  if (ctx.chunk_limbs <= 0 && chunk < (16ull << 20)) chunk = 16ull << 20;
+  if (chunk == 0) chunk = 1;
+
+  if (specs.size() < 2 || total <= chunk) {
+    ctx.batch_chunks = 1;
+    const int64_t t0 = now_ns();
+    Plan plan;
+    int s = plan.build(std::move(specs), ctx.ws);
+    if (!s) count_bytes(plan);
+    const int64_t t1 = now_ns();
+    if (!s) s = plan.upload(st);
+    const int64_t t2 = now_ns();
+    if (!s) s = plan.execute(st);
+    if (!s) s = plan.download_enqueue(st);
+    const int64_t t3 = now_ns();
+    if (!s) s = plan.download_finish(st);
+    const int64_t t4 = now_ns();
+    ctx.batch_ns[0] = t1 - t0;
+    ctx.batch_ns[1] = t2 - t1;
+    ctx.batch_ns[2] = t3 - t2;
+    ctx.batch_ns[3] = t4 - t3;
+    return s;
+  }
+
+  // chunks of consecutive whole products
+  std::vector<size_t> bounds{0};
+  uint64_t acc = 0;
+  for (size_t t = 0; t < specs.size(); ++t) {
+    acc += limbs[t];
+    if (acc >= chunk && t + 1 < specs.size()) {
+      bounds.push_back(t + 1);
+      acc = 0;
+    }
+  }
+  bounds.push_back(specs.size());
+  const size_t nchunks = bounds.size() - 1;
+  ctx.batch_chunks = (int64_t)nchunks;
+  int s = ensure_pipeline(ctx);
+  if (s) return s;
+  // the pipeline's streams start after the caller's earlier work
+  CU(cudaEventRecord(ctx.pipe_ev, st), "cudaEventRecord");
+  for (cudaStream_t ps : ctx.pipe_st) CU(cudaStreamWaitEvent(ps, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
+  CU(cudaStreamWaitEvent(ctx.pipe_in, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
+  CU(cudaStreamWaitEvent(ctx.pipe_out, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
+
+  // The caller's thread plans chunks and waits for finished ones; a
+  // submitter thread queues each chunk's copies and kernels, because queueing
+  // a copy can block the host until the copy engine takes it.
+  std::unique_ptr<Plan> plans[kPipeDepth];
+  size_t slot_chunk[kPipeDepth] = {};
+  bool slot_ok[kPipeDepth] = {};
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<size_t> queue;
+  size_t submitted = 0;  // chunks [0, submitted) have left the submitter
+  bool closing = false;
+  int sub_status = kOk;
+  std::string sub_msg;
+  int64_t sub_ns[2] = {0, 0};
+  std::thread submitter([&] {
+    cudaSetDevice(ctx.device);
+    for (;;) {
+      size_t c;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return !queue.empty() || closing; });
+        if (queue.empty()) return;
+        c = queue.front();
+        queue.pop_front();
+      }
+      const int w = (int)(c % kPipeDepth);
+      Plan* p = plans[w].get();
+      cudaStream_t ps = ctx.pipe_st[w];
+      const int64_t t0 = now_ns();
+      // copies in each direction in chunk order on their own stream; the
+      // kernels of neighbouring chunks may overlap (one chunk's tail fills
+      // in beside the next)
+      int r = p->upload(ctx.pipe_in);
+      if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_in[w], ctx.pipe_in), "cudaEventRecord");
+      const int64_t t1 = now_ns();
+      if (!r) r = cuda_status(cudaStreamWaitEvent(ps, ctx.pipe_ev_in[w], 0), "wait");
+      if (!r) r = p->execute(ps);
+      if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_exec[w], ps), "cudaEventRecord");
+      if (!r) r = cuda_status(cudaStreamWaitEvent(ctx.pipe_out, ctx.pipe_ev_exec[w], 0), "wait");
+      if (!r) r = p->download_enqueue(ctx.pipe_out);
+      if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_out[w], ctx.pipe_out), "cudaEventRecord");
+      const int64_t t2 = now_ns();
+      std::lock_guard<std::mutex> lk(mu);
+      sub_ns[0] += t1 - t0;
+      sub_ns[1] += t2 - t1;
+      if (r && !sub_status) {
+        sub_status = r;
+        sub_msg = last_error();
+      }
+      slot_ok[w] = r == kOk;
+      submitted = c + 1;
+      cv.notify_all();
+    }
+  });
+
+  // first error wins; a capacity error (some output did not fit) leaves
+  // every other result written, like an unchunked batch, so the chunks go on
+  int status = kOk;
+  bool stop = false;
+  auto finish = [&](int w) {
+    if (!plans[w]) return;
+    bool ok;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return submitted > slot_chunk[w]; });
+      ok = slot_ok[w];
+      if (sub_status) stop = true;
+    }
+    const int64_t t0 = now_ns();
+    int r = kOk;
+    if (ok) {
+      r = plans[w]->download_finish(ctx.pipe_out, ctx.pipe_ev_out[w]);
+    } else {  // wait for whatever was queued; results invalid
+      cudaStreamSynchronize(ctx.pipe_in);
+      cudaStreamSynchronize(ctx.pipe_st[w]);
+      cudaStreamSynchronize(ctx.pipe_out);
+    }
+    ctx.batch_ns[3] += now_ns() - t0;
+    if (r && !status) status = r;
+    if (r && r != kErrCapacity) stop = true;
+    plans[w].reset();
+  };
+  for (size_t c = 0; c < nchunks; ++c) {
+    const int w = (int)(c % kPipeDepth);
+    finish(w);  // the chunk that last used this workspace
+    if (stop) break;
+    std::vector<ProductSpec> part;
+    part.reserve(bounds[c + 1] - bounds[c]);
+    for (size_t t = bounds[c]; t < bounds[c + 1]; ++t) part.push_back(std::move(specs[t]));
+    plans[w].reset(new Plan);
+    const int64_t t0 = now_ns();
+    const int r = plans[w]->build(std::move(part), ctx.pipe_ws[w]);
+    ctx.batch_ns[0] += now_ns() - t0;
+    if (r) {
+      if (!status) status = r;
+      stop = true;
+      plans[w].reset();
+      break;
+    }
+    count_bytes(*plans[w]);
+    slot_chunk[w] = c;
+    std::lock_guard<std::mutex> lk(mu);
+    queue.push_back(c);
+    cv.notify_all();
+  }
+  // drain in chunk order (every chunk in flight is waited for, also on error)
+  for (size_t c = nchunks > (size_t)kPipeDepth ? nchunks - kPipeDepth : 0; c < nchunks; ++c)
+    finish((int)(c % kPipeDepth));
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    closing = true;
+    cv.notify_all();
+  }
+  submitter.join();
+  ctx.batch_ns[1] = sub_ns[0];
+  ctx.batch_ns[2] = sub_ns[1];
+  if (sub_status && (!status || status == kErrCapacity)) status = set_error(sub_status, sub_msg);
   return status;
 }
 

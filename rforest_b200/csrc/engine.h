@@ -9,6 +9,7 @@
 #include <functional>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mpzmm_internal.h"
@@ -62,18 +63,23 @@ struct Workspace {
   int32_t* d_sizes = nullptr;
   uint8_t* d_desc = nullptr;
   int* d_status = nullptr;  // nonzero: a kernel's bounded wait gave up
+  // pinned staging: only the inputs and outputs that cannot move straight
+  // between the caller's memory and the device pass through these
   uint64_t* h_limbs = nullptr;
   uint32_t* h_out = nullptr;
   int32_t* h_sizes = nullptr;
   uint8_t* h_desc = nullptr;
+  int* h_status = nullptr;  // pinned copy of d_status
   size_t cap_limbs = 0, cap_res = 0, cap_out = 0, cap_sizes = 0, cap_desc = 0;
   size_t hcap_limbs = 0, hcap_out = 0, hcap_sizes = 0, hcap_desc = 0;
   int64_t device_bytes = 0;
   // With a stream set, device buffers come from the stream-ordered memory
   // pool (cudaMallocAsync / cudaFreeAsync on that stream).
   cudaStream_t async_stream = nullptr;
-  // Ensures room for the given element counts; returns a status.
-  int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes);
+  // Ensures room for the given element counts (device buffers, then the
+  // pinned staging of limbs and output words); returns a status.
+  int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,
+              size_t stage_limbs, size_t stage_out_words);
   void release_device();  // device buffers only (pinned host buffers stay)
   void release();
   ~Workspace() { release(); }
@@ -101,7 +107,31 @@ struct Context {
   // filled by mpzmm_autotune
   int tc_pref[4][5] = {{-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1},
                        {-1, -1, -1, -1, -1}};
+  // pipelined one-shot batches: workspaces and streams of the chunks in
+  // flight (the first workspace is `ws`), created on first use
+  std::vector<Workspace*> pipe_ws;
+  std::vector<cudaStream_t> pipe_st;  // kernels, one stream per slot
+  cudaStream_t pipe_in = nullptr;     // every chunk's host->device copies, in order
+  cudaStream_t pipe_out = nullptr;    // every chunk's device->host copies, in order
+  cudaEvent_t pipe_ev = nullptr;
+  // per slot: its chunk's inputs on the device, its kernels done, its
+  // results on the host
+  std::vector<cudaEvent_t> pipe_ev_in, pipe_ev_exec, pipe_ev_out;
+  int64_t chunk_limbs = 0;  // input limbs per chunk; 0 = automatic
+  // last one-shot batch: host time of planning, input copies, launch
+  // queueing, waiting + results (ns); chunks; bytes host->device,
+  // device->host, and the parts of those that moved straight between the
+  // caller's pinned memory and the device
+  int64_t batch_ns[4] = {0, 0, 0, 0};
+  int64_t batch_chunks = 0;
+  int64_t batch_bytes[4] = {0, 0, 0, 0};
 };
+
+// Chunks in flight in a pipelined one-shot batch.
+constexpr int kPipeDepth = 4;
+// Largest host gap (limbs) between consecutive entries in one pinned range
+// that a copy run bridges instead of starting a new copy.
+constexpr int64_t kRunGapLimbs = 256;
 
 inline int tc_bucket_k(int k) {
   int b = 0;
@@ -126,6 +156,20 @@ void parallel_chunks(size_t n, size_t bytes, const std::function<void(size_t, si
 int ensure_setup(int device);
 void teardown();
 
+// Pinned host memory known to the library: transfers whose host side lies
+// wholly inside one such range go straight to or from the caller's memory.
+int host_alloc(size_t bytes, void** out);
+int host_free(void* p);
+int host_register(void* p, size_t bytes);
+int host_unregister(void* p);
+bool host_range_pinned(const void* p, size_t bytes);
+// Snapshot of the known ranges (sorted by start) and lookups in it.
+std::vector<std::pair<uintptr_t, size_t>> pinned_ranges();
+bool in_ranges(const std::vector<std::pair<uintptr_t, size_t>>& v, const void* p, size_t bytes);
+// End address of the range holding [p, p + bytes), 0 if none does.
+uintptr_t range_end(const std::vector<std::pair<uintptr_t, size_t>>& v, const void* p,
+                    size_t bytes);
+
 class Plan {
  public:
   static constexpr int kStages = 4;
@@ -133,16 +177,30 @@ class Plan {
   // Computes parameters, descriptors and launch groups, and reserves device
   // and pinned host buffers in `ws` (the plan's own workspace if null).
   int build(std::vector<ProductSpec> prods, Workspace* ws = nullptr);
-  // Gathers input limbs into pinned memory and copies them (and the
-  // descriptors) to the device.
+  // Copies the input limbs (and the descriptors) to the device: straight
+  // from the caller's memory where it is pinned memory known to the library,
+  // through the pinned staging buffer otherwise.
   int upload(cudaStream_t st);
   // Runs split+fwd NTT, contraction, inverse NTT, CRT+recompose.  With
   // graph mode on (and timing off) the launches are captured into a CUDA
   // graph on the first call and replayed as one graph launch afterwards.
   int execute(cudaStream_t st);
   void set_graph(bool on) { use_graph_ = on; }
-  // Copies outputs back and writes them to the output references.
+  // Copies outputs back and writes them to the output references:
+  // download_enqueue queues the device->host copies, download_finish waits
+  // (for `done` when given, else for the whole stream) and writes sizes and
+  // staged limbs to the destinations.
   int download(cudaStream_t st);
+  int download_enqueue(cudaStream_t st);
+  int download_finish(cudaStream_t st, cudaEvent_t done = nullptr);
+  // bytes moved per upload / download, and the parts of them that go
+  // straight between pinned caller memory and the device
+  uint64_t upload_bytes() const { return n_limbs_ * 8 + desc_bytes_; }
+  uint64_t download_bytes() const {
+    return n_out_words_ * 4 + (inv_.empty() ? 0 : outs_.size() * 4) + sizeof(int);
+  }
+  uint64_t direct_in_bytes() const { return direct_in_limbs_ * 8; }
+  uint64_t direct_out_bytes() const { return direct_out_words_ * 4; }
 
   int64_t launches_per_execute() const { return launches_; }
   // Stage timing with CUDA events recorded on the execute stream: stages are
@@ -182,6 +240,22 @@ class Plan {
   std::vector<CtaItem> cta_items_;
   std::vector<OutRef> outs_;          // flattened output references
   std::vector<int64_t> out_word_off_; // per output entry (words)
+  std::vector<int32_t> out_limbs_;    // per output entry: limbs the device writes
+  // host<->device transfer runs: `rows` rows of `n` elements (limbs in,
+  // words out) between host address `host` (rows `pitch` elements apart)
+  // and device element offset `dev` (rows back to back); staged runs go
+  // through the pinned staging buffer at element offset `stage`
+  struct Run {
+    const void* host;
+    uint64_t dev, n, stage;
+    bool direct;
+    uint64_t rows, pitch;
+  };
+  std::vector<Run> in_runs_, out_runs_;
+  std::vector<int64_t> out_stage_;    // per output entry: staging word offset, -1 if direct
+  uint64_t stage_limbs_ = 0, stage_out_words_ = 0;
+  uint64_t direct_in_limbs_ = 0, direct_out_words_ = 0;
+  void plan_transfers();
   std::vector<uint8_t> zero_prod_;    // product is identically zero
 
   uint64_t n_limbs_ = 0, n_res_ = 0, n_out_words_ = 0;
@@ -208,5 +282,15 @@ class Plan {
   cudaGraphExec_t graph_exec_ = nullptr;
   int launch_all(cudaStream_t st, bool timed);
 };
+
+// One-shot batch on the shared workspace: build, upload, execute, download.
+// Batches with more input than one chunk are split into chunks of whole
+// products that run as a pipeline over kPipeDepth workspaces: all chunks'
+// host->device copies go in order on one stream, all device->host copies on
+// another, and each chunk's kernels on its slot's stream between the two,
+// so one chunk's inputs move in while earlier chunks compute and return
+// their results (two copy streams also keep the copy directions on
+// separate copy queues).  Returns when every result is written.
+int run_batch(std::vector<ProductSpec> specs, cudaStream_t st);
 
 }  // namespace mpzmm

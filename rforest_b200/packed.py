@@ -14,6 +14,17 @@ from typing import Iterable, List, Sequence
 import numpy as np
 
 
+def bit_length_u64(x: np.ndarray) -> np.ndarray:
+    """Exact bit length of each uint64 (0 for 0)."""
+    x = np.array(x, dtype=np.uint64, copy=True)
+    b = np.zeros(x.shape, dtype=np.int64)
+    for s in (32, 16, 8, 4, 2, 1):
+        m = x >= np.uint64(1 << s)
+        b[m] += s
+        x[m] >>= np.uint64(s)
+    return b + (x > 0)
+
+
 @dataclass
 class Packed:
     limbs: np.ndarray  # uint64
@@ -29,6 +40,15 @@ class Packed:
 
     def max_limbs(self) -> int:
         return int(self.nlimbs.max()) if len(self) else 0
+
+    def max_bits(self) -> int:
+        """Largest bit length of an entry's magnitude (0 if all are zero)."""
+        n = self.nlimbs
+        nz = n > 0
+        if not nz.any():
+            return 0
+        top = self.limbs[self.offs[nz] + n[nz] - 1]
+        return int((64 * (n[nz] - 1) + bit_length_u64(top)).max())
 
     def entry(self, e: int) -> int:
         """Entry ``e`` as a Python int."""
