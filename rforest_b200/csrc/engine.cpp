@@ -472,7 +472,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     const uint64_t N = (uint64_t)1 << lgN;
     const uint64_t poly = (uint64_t)P * N;
     // the contraction addresses a product's residues with 32-bit offsets
-    if (((uint64_t)m * k + (uint64_t)k * n + (uint64_t)m * n) * poly >= (1ull << 32))
+    if (((uint64_t)m * k + (uint64_t)k * n + (uint64_t)m * n) * poly + 16 >= (1ull << 32))
       return set_error(kErrTooLarge, "product needs more than 2^32 residue words");
     ProdDesc pd;
     pd.m = (uint16_t)m;
@@ -481,10 +481,13 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     pd.lgN = (uint16_t)lgN;
     pd.P = (uint16_t)P;
     pd.pad = (uint16_t)((m >= 3 ? 2 : 0) + (n >= 3 ? 1 : 0));  // contraction tile
+    n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.a_res = n_res_;
     n_res_ += (uint64_t)m * k * poly;
+    n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.b_res = n_res_;
     n_res_ += (uint64_t)k * n * poly;
+    n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.c_res = n_res_;
     n_res_ += (uint64_t)m * n * poly;
     for (int side = 0; side < 2; ++side) {

@@ -374,6 +374,38 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
   return (neg && v) ? p - v : v;
 }
 
+// 2^L consecutive points reduced from [0, 4p) to [0, p), vector stores
+template <int L>
+__device__ __forceinline__ void store_points(uint32_t* dst, uint32_t* a, uint32_t p) {
+  const uint32_t p2 = 2 * p;
+#pragma unroll
+  for (int q = 0; q < (1 << L); ++q) {
+    const uint32_t v = reduce_2p(a[q], p2);
+    a[q] = v >= p ? v - p : v;
+  }
+  if (L == 3) {
+    reinterpret_cast<uint4*>(dst)[0] = make_uint4(a[0], a[1], a[2], a[3]);
+    reinterpret_cast<uint4*>(dst)[1] = make_uint4(a[4], a[5], a[6], a[7]);
+  } else if (L == 2) {
+    reinterpret_cast<uint4*>(dst)[0] = make_uint4(a[0], a[1], a[2], a[3]);
+  } else {
+    reinterpret_cast<uint2*>(dst)[0] = make_uint2(a[0], a[1]);
+  }
+}
+
+template <int LP>
+__device__ __forceinline__ void fwd_last_pass(const uint32_t* s, uint32_t* out, bool valid,
+                                              int lgN, int last_s0, int tt, int TS,
+                                              const uint2* __restrict__ tw, uint32_t p) {
+  for (int g = tt; g < ((1 << lgN) >> LP); g += TS) {
+    uint32_t a[1 << LP];
+#pragma unroll
+    for (int q = 0; q < (1 << LP); ++q) a[q] = s[smi((g << LP) + q)];
+    fwd_group<LP>(a, last_s0, g, tw, p);
+    if (valid) store_points<LP>(out + (g << LP), a, p);
+  }
+}
+
 template <int D, bool TEAM>
 __global__ void __launch_bounds__(kFwdThreads, 3)
 k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
@@ -412,6 +444,7 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   for (int j = 0; j < P; ++j) {
     const uint32_t p = c_primes[j].p;
     const uint2* tw = twf + (size_t)j * kTwStride;
+    uint32_t* out = res + d.res_off + (uint64_t)j * (uint64_t)N;
     for (int g = tt; g < ng0; g += TS) {
       uint32_t a[8];
 #pragma unroll
@@ -422,28 +455,143 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
         a[q] = digits_residue<D>(dg[q], j, neg);
       }
       fwd_group<3>(a, 0, 0, tw, p);
+      if (lgN == 3) {  // the only pass: eight consecutive points, straight out
+        if (valid) store_points<3>(out, a, p);
+      } else {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) s[smi(q * ng0 + g)] = a[q];
+        for (int q = 0; q < 8; ++q) s[smi(q * ng0 + g)] = a[q];
+      }
     }
+    if (lgN == 3) continue;  // uniform per CTA
     __syncthreads();
-    for (int s0 = 3; s0 < lgN; s0 += 3) {
-      const int Lp = (lgN - s0) < 3 ? (lgN - s0) : 3;
-      smem_pass<3, true>(s, lgN, s0, Lp, tt, TS, tw, p);
+    const int last_s0 = ((lgN - 1) / 3) * 3;
+    for (int s0 = 3; s0 < last_s0; s0 += 3) {
+      smem_pass<3, true>(s, lgN, s0, 3, tt, TS, tw, p);
       __syncthreads();
     }
-    if (valid) {
-      uint32_t* out = res + d.res_off + (uint64_t)j * (uint64_t)N;
-      const uint32_t p2 = 2 * p;
-      for (int x = tt; x < N; x += TS) {
-        uint32_t v = reduce_2p(s[smi(x)], p2);
-        out[x] = v >= p ? v - p : v;
+    // the last pass works on groups of 2^LP consecutive points: reduced and
+    // stored straight from registers with vector stores
+    switch (lgN - last_s0) {
+      case 1: fwd_last_pass<1>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
+      case 2: fwd_last_pass<2>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
+      default: fwd_last_pass<3>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
+    }
+    __syncthreads();  // before the next prime's first pass overwrites s
+  }
+}
+
+// Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
+//
+// The last forward pass (stages last_s0 .. lgN-1, LP = lgN - last_s0 of
+// them) works on groups of 2^LP consecutive points, so its inverse reads
+// each group straight from global memory with one or two vector loads and
+// only then goes to shared memory.  In a team CTA every thread owns exactly
+// eight of those points per prime, and the next prime's eight are loaded
+// into registers before the current prime's passes run, so the loads
+// overlap the arithmetic instead of stalling the warps.
+
+template <int L>
+__device__ __forceinline__ void load_points(const uint32_t* src, uint32_t* a) {
+  if (L == 3) {
+    const uint4 u = *reinterpret_cast<const uint4*>(src);
+    const uint4 v = *reinterpret_cast<const uint4*>(src + 4);
+    a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w;
+    a[4] = v.x; a[5] = v.y; a[6] = v.z; a[7] = v.w;
+  } else if (L == 2) {
+    const uint4 u = *reinterpret_cast<const uint4*>(src);
+    a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w;
+  } else {
+    const uint2 u = *reinterpret_cast<const uint2*>(src);
+    a[0] = u.x; a[1] = u.y;
+  }
+}
+
+// the groups of the last forward pass (2^LP points each) in registers:
+// inverse stages, then into shared memory
+template <int LP>
+__device__ __forceinline__ void inv_last_pass(uint32_t* s, const uint32_t* a_in, int g,
+                                              int last_s0, const uint2* tw, uint32_t p) {
+  uint32_t a[1 << LP];
+#pragma unroll
+  for (int q = 0; q < (1 << LP); ++q) a[q] = a_in[q];
+  inv_group<LP>(a, last_s0, g, tw, p);
+#pragma unroll
+  for (int q = 0; q < (1 << LP); ++q) s[smi((g << LP) + q)] = a[q];
+}
+
+template <int LP, bool TEAM>
+__device__ __forceinline__ void inv_run(uint32_t* s, uint32_t* __restrict__ res, uint64_t off,
+                                        bool valid, int lgN, int P, int tt, int TS,
+                                        const uint2* __restrict__ twi) {
+  const int N = 1 << lgN;
+  const int last_s0 = lgN - LP;
+  constexpr int GT = 8 >> LP;  // groups per thread in a team CTA
+  uint32_t nx[8];               // team: the next prime's points
+  if (TEAM && valid) {
+#pragma unroll
+    for (int k = 0; k < GT; ++k) load_points<LP>(res + off + ((tt + k * TS) << LP), nx + (k << LP));
+  }
+  for (int j = 0; j < P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = twi + (size_t)j * kTwStride;
+    uint32_t* io = res + off + (uint64_t)j * (uint64_t)N;
+    if (last_s0 == 0) {
+      // lgN = 3: one pass, global -> registers -> global
+      if (TEAM && valid) {
+        uint32_t a[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[q] = nx[q];
+        if (j + 1 < P) load_points<3>(io + N, nx);
+        inv_group<3>(a, 0, 0, tw, p);
+        uint4* o = reinterpret_cast<uint4*>(io);
+        o[0] = make_uint4(a[0], a[1], a[2], a[3]);
+        o[1] = make_uint4(a[4], a[5], a[6], a[7]);
+      }
+      continue;
+    }
+    if (TEAM) {
+      uint32_t a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = valid ? nx[q] : 0u;
+      if (valid && j + 1 < P) {
+#pragma unroll
+        for (int k = 0; k < GT; ++k)
+          load_points<LP>(io + N + ((tt + k * TS) << LP), nx + (k << LP));
+      }
+#pragma unroll
+      for (int k = 0; k < GT; ++k) inv_last_pass<LP>(s, a + (k << LP), tt + k * TS, last_s0, tw, p);
+    } else {
+      for (int g = tt; g < (N >> LP); g += TS) {
+        uint32_t a[1 << LP];
+        if (valid) {
+          load_points<LP>(io + (g << LP), a);
+        } else {
+#pragma unroll
+          for (int q = 0; q < (1 << LP); ++q) a[q] = 0u;
+        }
+        inv_last_pass<LP>(s, a, g, last_s0, tw, p);
+      }
+    }
+    __syncthreads();
+    for (int s0 = last_s0 - 3; s0 >= 3; s0 -= 3) {
+      smem_pass<3, false>(s, lgN, s0, 3, tt, TS, tw, p);
+      __syncthreads();
+    }
+    // first forward pass (stages 0..2) inverted, straight to global memory
+    for (int g = tt; g < (N >> 3); g += TS) {
+      uint32_t a[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) a[q] = s[smi(q * (N >> 3) + g)];
+      inv_group<3>(a, 0, 0, tw, p);
+      if (valid) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) io[q * (N >> 3) + g] = a[q];  // in [0, 2p)
       }
     }
     __syncthreads();
   }
 }
 
-// Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
 template <bool TEAM>
 __global__ void __launch_bounds__(kFwdThreads)
 k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
@@ -461,29 +609,10 @@ k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   uint32_t* s = sm + team * (N + (N >> 5));
   const uint64_t off = valid ? descs[idx[item.first + team]].res_off : 0;
   const int last_s0 = ((lgN - 1) / 3) * 3;  // start of the last forward pass
-  for (int j = 0; j < P; ++j) {
-    const uint32_t p = c_primes[j].p;
-    const uint2* tw = twi + (size_t)j * kTwStride;
-    uint32_t* io = res + off + (uint64_t)j * (uint64_t)N;
-    for (int x = tt; x < N; x += TS) s[smi(x)] = valid ? io[x] : 0u;
-    __syncthreads();
-    for (int s0 = last_s0; s0 >= 3; s0 -= 3) {
-      const int Lp = (lgN - s0) < 3 ? (lgN - s0) : 3;
-      smem_pass<3, false>(s, lgN, s0, Lp, tt, TS, tw, p);
-      __syncthreads();
-    }
-    // first forward pass (stages 0..2) inverted, straight to global memory
-    for (int g = tt; g < (N >> 3); g += TS) {
-      uint32_t a[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) a[q] = s[smi(q * (N >> 3) + g)];
-      inv_group<3>(a, 0, 0, tw, p);
-      if (valid) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) io[q * (N >> 3) + g] = a[q];  // in [0, 2p)
-      }
-    }
-    __syncthreads();
+  switch (lgN - last_s0) {
+    case 1: inv_run<1, TEAM>(s, res, off, valid, lgN, P, tt, TS, twi); break;
+    case 2: inv_run<2, TEAM>(s, res, off, valid, lgN, P, tt, TS, twi); break;
+    default: inv_run<3, TEAM>(s, res, off, valid, lgN, P, tt, TS, twi); break;
   }
 }
 
