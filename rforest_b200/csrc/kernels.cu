@@ -647,25 +647,51 @@ __device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, uint
     frac += (uint64_t)y[j] * c_crt.fq[j];
   }
   const uint32_t q = (uint32_t)((frac + (1ull << 57)) >> 58);  // nearest integer
+  // sum_j y_j (M_P / p_j) in base-2^30 columns (M_P / p_j has P - 1 digits):
+  // products below 2^60, at most 16 per column, no carries inside the sum
+  uint64_t acc[P];
 #pragma unroll
-  for (int w = 0; w < P; ++w) X[w] = 0;
+  for (int w = 0; w < P; ++w) acc[w] = 0;
 #pragma unroll
-  for (int j = 0; j < P; ++j) {
-    uint64_t cy = 0;
+  for (int j = 0; j < P; ++j)
 #pragma unroll
-    for (int w = 0; w < P; ++w) {
-      const uint64_t t = (uint64_t)y[j] * c_crt.mop[P][j][w] + X[w] + cy;
-      X[w] = (uint32_t)t;
-      cy = t >> 32;
-    }
-  }
-  uint32_t br = 0;  // X -= q M_P (mod 2^(32P))
+    for (int w = 0; w + 1 < P; ++w) acc[w] += (uint64_t)y[j] * c_crt.mop30[P][j][w];
+  // digits: carry-normalise (column + carry < 2^64), then subtract q M_P with
+  // a signed borrow; the top digit is 0 for X >= 0 and -1 for X < 0
+  uint32_t dg[P];
+  uint64_t cy = 0;
 #pragma unroll
   for (int w = 0; w < P; ++w) {
-    const uint64_t t = (uint64_t)q * c_crt.M[P][w] + br;
-    const uint32_t lo = (uint32_t)t;
-    br = (uint32_t)(t >> 32) + (X[w] < lo ? 1u : 0u);
-    X[w] -= lo;
+    const uint64_t t = acc[w] + cy;
+    dg[w] = (uint32_t)t & 0x3fffffffu;
+    cy = t >> 30;
+  }
+  int64_t b = 0;
+#pragma unroll
+  for (int w = 0; w < P; ++w) {
+    const int64_t e = (int64_t)dg[w] - (int64_t)q * (int64_t)c_crt.M30[P][w] + b;
+    dg[w] = (uint32_t)e & 0x3fffffffu;
+    b = e >> 30;  // arithmetic: floor division
+  }
+  const bool neg = ((int64_t)cy + b) < 0;
+  // repack the 30P bits to P 32-bit words of the two's complement value
+  uint64_t buf = 0;
+  int bits = 0, wi = 0;
+#pragma unroll
+  for (int w = 0; w < P; ++w) {
+    buf |= (uint64_t)dg[w] << bits;
+    bits += 30;
+    if (bits >= 32) {
+      X[wi++] = (uint32_t)buf;
+      buf >>= 32;
+      bits -= 32;
+    }
+  }
+  const uint32_t fill = neg ? 0xffffffffu : 0u;
+#pragma unroll
+  for (int w = 0; w < P; ++w) {
+    if (w < wi) continue;
+    X[w] = (w == wi) ? ((uint32_t)buf | (fill << bits)) : fill;
   }
 }
 

@@ -41,11 +41,14 @@ struct PrimeConst {
 //     X = sum_j y_j (M_P / p_j) - q M_P,   y_j = x_j (M_P / p_j)^{-1} mod p_j,
 // where q is sum_j y_j / p_j rounded to the nearest integer (computed in
 // 2^-58 fixed point; the planner keeps |X| < M_P / 4, so the rounding has a
-// margin of 1/4 against a fixed-point error below 2^-24).
+// margin of 1/4 against a fixed-point error below 2^-24).  The sums run in
+// base 2^30: every y_j d product is below 2^60, so a column of up to 16 of
+// them fits one 64-bit accumulator without carry handling.
 struct CrtConst {
   uint32_t M[kMaxPrimes + 1][kMaxCrtWords];          // M_P, little-endian words
   int Mwords[kMaxPrimes + 1];
-  uint32_t mop[kMaxPrimes + 1][kMaxPrimes][kMaxPrimes];  // M_P / p_j, P words
+  uint32_t M30[kMaxPrimes + 1][kMaxPrimes];          // M_P, base-2^30 digits (P of them)
+  uint32_t mop30[kMaxPrimes + 1][kMaxPrimes][kMaxPrimes];  // M_P / p_j, base-2^30 digits
   // Montgomery form (times 2^32) of 2^32 N^{-1} (M_P / p_j)^{-1} mod p_j for
   // N = 2^lgN: removes the contraction's 2^-32 and the inverse transform's N
   uint32_t cm[kMaxPrimes + 1][kMaxLgN + 1][kMaxPrimes];

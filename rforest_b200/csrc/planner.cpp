@@ -96,6 +96,25 @@ void mul_small(std::vector<uint32_t>& x, uint32_t v) {
   if (cy) x.push_back((uint32_t)cy);
 }
 
+// base-2^32 little-endian words -> base-2^30 digits (no trailing zero digits)
+std::vector<uint32_t> to_base30(const std::vector<uint32_t>& w32) {
+  std::vector<uint32_t> out;
+  unsigned __int128 buf = 0;
+  int bits = 0;
+  for (uint32_t w : w32) {
+    buf |= (unsigned __int128)w << bits;
+    bits += 32;
+    while (bits >= 30) {
+      out.push_back((uint32_t)(buf & 0x3fffffffu));
+      buf >>= 30;
+      bits -= 30;
+    }
+  }
+  if (bits > 0) out.push_back((uint32_t)buf);
+  while (!out.empty() && out.back() == 0) out.pop_back();
+  return out;
+}
+
 Moduli* g_moduli = nullptr;
 std::once_flag g_once;
 
@@ -146,6 +165,8 @@ void build(Moduli& M) {
     int words = (int)acc.size();
     M.crt.Mwords[P] = words;
     for (int q = 0; q < words && q < kMaxCrtWords; ++q) M.crt.M[P][q] = acc[q];
+    const std::vector<uint32_t> m30 = to_base30(acc);
+    for (int w = 0; w < kMaxPrimes; ++w) M.crt.M30[P][w] = w < (int)m30.size() ? m30[w] : 0u;
     int top = 31;
     while (!((acc.back() >> top) & 1u)) --top;
     M.mbits[P] = 32 * (words - 1) + top;  // floor(log2 M)
@@ -162,8 +183,9 @@ void build(Moduli& M) {
         mul_small(mop, M.p[a]);
         mop_mod = mop_mod * (M.p[a] % pj) % pj;
       }
+      const std::vector<uint32_t> m30 = to_base30(mop);
       for (int w = 0; w < kMaxPrimes; ++w)
-        M.crt.mop[P][j][w] = w < (int)mop.size() ? mop[w] : 0u;
+        M.crt.mop30[P][j][w] = w < (int)m30.size() ? m30[w] : 0u;
       const uint64_t inv = powmod(mop_mod, pj - 2, pj);
       const uint64_t r32 = (((uint64_t)1) << 32) % pj;
       for (int lg = 0; lg <= kMaxLgN; ++lg) {
