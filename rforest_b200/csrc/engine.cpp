@@ -566,6 +566,9 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       id.res_off = pd.c_res + (uint64_t)e * poly;
       id.out_word = n_out_words_;
       id.out_words = (uint32_t)(2 * prm.out_limbs);
+      // the CRT kernel's bit positions are 31-bit integers
+      if ((uint64_t)id.out_words * 32 + 32 * (uint64_t)P + (uint64_t)r >= (1ull << 31))
+        return set_error(kErrTooLarge, "output entry above 2^31 bits");
       out_word_off_.push_back((int64_t)n_out_words_);
       out_limbs_.push_back((int32_t)prm.out_limbs);
       n_out_words_ += id.out_words;

@@ -695,6 +695,19 @@ __device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, uint
   }
 }
 
+// floor(x / d) for x < 2^31: a multiply-high by floor((2^32 - 1) / d) is at
+// most 2 below the quotient, then at most two corrections
+struct FastDiv {
+  uint32_t d, m;
+  __device__ explicit FastDiv(uint32_t d_) : d(d_), m(0xffffffffu / d_) {}
+  __device__ __forceinline__ uint32_t operator()(uint32_t x) const {
+    uint32_t q = __umulhi(x, m);
+    if ((q + 1) * d <= x) ++q;
+    if ((q + 1) * d <= x) ++q;
+    return q;
+  }
+};
+
 template <int P>
 __global__ void __launch_bounds__(32 * kCrtWarps)
 k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
@@ -707,22 +720,25 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
   const int slot = blockIdx.x * kCrtWarps + warp;
   if (slot >= count) return;  // whole warp; no block-wide barrier below
   const InvDesc d = descs[idx[slot]];
-  const int64_t r = d.r;
-  const int64_t W = d.out_words;
-  const int64_t ncoef = d.ncoef;
+  // bit positions fit 31 bits (an entry's words times 32 stays below 2^31),
+  // so index arithmetic is 32-bit and the divisions by r are multiply-highs
+  const int r = (int)d.r;
+  const FastDiv divr((uint32_t)r);
+  const int W = (int)d.out_words;
+  const int ncoef = (int)d.ncoef;
   uint32_t* o = out + d.out_word;
   uint32_t* sU = sm + warp * (cmax * P);  // word q of tile coefficient c at [q * cmax + c]
 
   int hi_prev = 0, carry = 0;
   int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
   uint32_t topval = 0;
-  for (int64_t w0 = 0; w0 < W; w0 += kCrtTileWords) {
-    int64_t lo_i = 0;
-    if (32 * w0 - 32 * (int64_t)P > 0) lo_i = (32 * w0 - 32 * (int64_t)P + r - 1) / r;
-    int64_t hi_i = (32 * (w0 + kCrtTileWords) - 1) / r;
+  for (int w0 = 0; w0 < W; w0 += kCrtTileWords) {
+    int lo_i = 0;
+    if (32 * w0 > 32 * P) lo_i = (int)divr((uint32_t)(32 * w0 - 32 * P + r - 1));
+    int hi_i = (int)divr((uint32_t)(32 * (w0 + kCrtTileWords) - 1));
     if (hi_i > ncoef - 1) hi_i = ncoef - 1;
-    const int64_t ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
-    for (int64_t c = lane; c < ncf; c += 32) {
+    const int ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
+    for (int c = lane; c < ncf; c += 32) {
       uint32_t X[P];
       crt_coeff<P>(res, d.res_off, d.lgN, lo_i + c, X);
 #pragma unroll
@@ -730,27 +746,27 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
     }
     __syncwarp();
     for (int st = 0; st < kCrtSteps; ++st) {
-      const int64_t w = w0 + st * 32 + lane;
+      const int w = w0 + st * 32 + lane;
       const bool active = w < W;
       int64_t sw = 0;
       if (active) {
-        int64_t ia = lo_i;
-        if (32 * w - 32 * (int64_t)P > 0) {
-          const int64_t t = (32 * w - 32 * (int64_t)P + r - 1) / r;
+        int ia = lo_i;
+        if (32 * w > 32 * P) {
+          const int t = (int)divr((uint32_t)(32 * w - 32 * P + r - 1));
           if (t > ia) ia = t;
         }
-        int64_t ib = (32 * w + 31) / r;
+        int ib = (int)divr((uint32_t)(32 * w + 31));
         if (ib > hi_i) ib = hi_i;
-        for (int64_t i = ia; i <= ib; ++i) {
-          const int64_t c = i - lo_i;
-          const int64_t bi = i * r;
-          const int64_t dd = 32 * w - bi;
+        for (int i = ia; i <= ib; ++i) {
+          const int c = i - lo_i;
+          const int bi = i * r;
+          const int dd = 32 * w - bi;
           const uint32_t* U = sU + c;  // word q at U[q * cmax]
           uint32_t slice;
           if (dd < 0) {
             slice = U[0] << (uint32_t)(-dd);
           } else {
-            const int64_t q = dd >> 5;
+            const int q = dd >> 5;
             const uint32_t sh = (uint32_t)(dd & 31);
             const uint32_t lo = q < P ? U[q * cmax] : 0u;
             const uint32_t hi = q + 1 < P ? U[(q + 1) * cmax] : 0u;
