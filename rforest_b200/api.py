@@ -214,14 +214,17 @@ class Batch:
             bufs = [(a, b, c) for (a, b), c in zip(ins, outs)]
         self.holders = [_Holder(*p, bufs=bb) for p, bb in zip(products, bufs)]
         self.arr = (_lib.Product * len(self.holders))(*[h.struct for h in self.holders])
+        # the results are views of the output arrays: made once, valid after every run
+        self.results = [h.result() for h in self.holders]
 
     def run(self, stream=None) -> List[Packed]:
         _lib.check(_lib.lib().mpzmm_matmul_batch(len(self.holders), self.arr,
                                                  _stream_arg(stream)))
-        return [h.result() for h in self.holders]
+        return self.results
 
     def close(self) -> None:
         self.holders = []
+        self.results = []
         self.arr = None
         if self.arena is not None:
             self.arena.close()

@@ -38,27 +38,11 @@ int cuda_status(cudaError_t e, const char* what) {
   } while (0)
 
 int64_t bit_length(const EntryRef& e) {
-  const int64_t n = e.size < 0 ? -(int64_t)e.size : e.size;
-  if (n == 0) return 0;
-  uint64_t top = e.d[n - 1];
-  int b = 0;
-  while (top) {
-    ++b;
-    top >>= 1;
-  }
+  int64_t i = (e.size < 0 ? -(int64_t)e.size : e.size) - 1;
   // a non-normalised top limb of zero is tolerated: scan down
-  if (b == 0) {
-    int64_t i = n - 1;
-    while (i >= 0 && e.d[i] == 0) --i;
-    if (i < 0) return 0;
-    uint64_t t = e.d[i];
-    while (t) {
-      ++b;
-      t >>= 1;
-    }
-    return 64 * i + b;
-  }
-  return 64 * (n - 1) + b;
+  while (i >= 0 && e.d[i] == 0) --i;
+  if (i < 0) return 0;
+  return 64 * i + (64 - __builtin_clzll(e.d[i]));
 }
 
 }  // namespace
@@ -416,6 +400,55 @@ int64_t estimate_device_bytes(const ProductSpec& ps) {
   return limbs * 8 + res + out + desc;
 }
 
+// Checks one product, finds its operands' bit lengths and its transform
+// parameters; returns a status (with the message in *msg when asked).
+static int plan_product(const ProductSpec& ps, Params* prm, std::string* msg) {
+  auto fail = [&](int code, const std::string& m) {
+    if (msg) *msg = m;
+    return code;
+  };
+  const int m = ps.m, k = ps.k, n = ps.n;
+  if (m < 0 || k < 0 || n < 0) return fail(kErrArg, "negative dimension");
+  if ((int64_t)ps.a.size() != (int64_t)m * k || (int64_t)ps.b.size() != (int64_t)k * n ||
+      (int64_t)ps.c.size() != (int64_t)m * n)
+    return fail(kErrArg, "entry count does not match the dimensions");
+  if (m > 65535 || k > 65535 || n > 65535) return fail(kErrTooLarge, "dimension > 65535");
+  int64_t a_bits = 0, b_bits = 0;
+  for (int side = 0; side < 2; ++side) {
+    const auto& ents = side ? ps.b : ps.a;
+    int64_t& bits = side ? b_bits : a_bits;
+    // only the longest entries can hold the largest bit length: read their
+    // top limbs (each read of a caller's limb is a likely cache miss, so
+    // they are prefetched together first), and scan everything only when
+    // none of those is normalised
+    int64_t max_nl = 0;
+    for (const auto& e : ents) {
+      if (e.size != 0 && e.d == nullptr) return fail(kErrArg, "null limb pointer");
+      const int64_t nl = e.size < 0 ? -(int64_t)e.size : e.size;
+      if (nl > max_nl) max_nl = nl;
+    }
+    if (!max_nl) continue;
+    for (const auto& e : ents)
+      if ((e.size < 0 ? -(int64_t)e.size : e.size) == max_nl)
+        __builtin_prefetch(e.d + max_nl - 1);
+    for (const auto& e : ents) {
+      if ((e.size < 0 ? -(int64_t)e.size : e.size) != max_nl) continue;
+      const int64_t b = bit_length(e);
+      if (b > bits) bits = b;
+    }
+    if (bits <= 64 * (max_nl - 1))
+      for (const auto& e : ents) {
+        const int64_t b = bit_length(e);
+        if (b > bits) bits = b;
+      }
+  }
+  if (!choose_params(a_bits, b_bits, m, k, n, prm))
+    return fail(kErrTooLarge, "product too large for a single transform (entries of " +
+                                  std::to_string(a_bits) + " and " + std::to_string(b_bits) +
+                                  " bits)");
+  return kOk;
+}
+
 int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   if (built_) return set_error(kErrState, "plan already built");
   prods_ = std::move(prods);
@@ -432,31 +465,28 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   uintptr_t run_pinned_end = 0;        // end of the pinned range of the current run (0: none)
   const auto pinned = pinned_ranges();
   in_runs_.clear();
+  // pass 1, across host threads: checks, operand bit lengths, parameters
+  // (independent per product); the first failing product's error is then
+  // reported from this thread
+  std::vector<int> bad(prods_.size(), 0);
+  {
+    size_t work = 0;
+    for (const auto& ps : prods_) work += ps.a.size() + ps.b.size();
+    parallel_chunks(prods_.size(), work * 4096, [&](size_t lo, size_t hi) {
+      for (size_t t = lo; t < hi; ++t) bad[t] = plan_product(prods_[t], &params_[t], nullptr);
+    });
+  }
+  for (size_t t = 0; t < prods_.size(); ++t)
+    if (bad[t]) {
+      std::string msg;
+      plan_product(prods_[t], &params_[t], &msg);
+      return set_error(bad[t], msg);
+    }
+  // pass 2, in order: offsets and descriptors
   for (size_t t = 0; t < prods_.size(); ++t) {
     ProductSpec& ps = prods_[t];
     const int m = ps.m, k = ps.k, n = ps.n;
-    if (m < 0 || k < 0 || n < 0) return set_error(kErrArg, "negative dimension");
-    if ((int64_t)ps.a.size() != (int64_t)m * k || (int64_t)ps.b.size() != (int64_t)k * n ||
-        (int64_t)ps.c.size() != (int64_t)m * n)
-      return set_error(kErrArg, "entry count does not match the dimensions");
-    if (m > 65535 || k > 65535 || n > 65535) return set_error(kErrTooLarge, "dimension > 65535");
-    int64_t a_bits = 0, b_bits = 0;
-    for (auto& e : ps.a) {
-      if (e.size != 0 && e.d == nullptr) return set_error(kErrArg, "null limb pointer");
-      int64_t b = bit_length(e);
-      if (b > a_bits) a_bits = b;
-    }
-    for (auto& e : ps.b) {
-      if (e.size != 0 && e.d == nullptr) return set_error(kErrArg, "null limb pointer");
-      int64_t b = bit_length(e);
-      if (b > b_bits) b_bits = b;
-    }
-    Params prm;
-    if (!choose_params(a_bits, b_bits, m, k, n, &prm))
-      return set_error(kErrTooLarge, "product too large for a single transform (entries of " +
-                                         std::to_string(a_bits) + " and " +
-                                         std::to_string(b_bits) + " bits)");
-    params_[t] = prm;
+    const Params prm = params_[t];
     const uint64_t first_out = out_entry;
     for (auto& c : ps.c) outs_.push_back(c);
     out_entry += ps.c.size();
@@ -490,6 +520,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.c_res = n_res_;
     n_res_ += (uint64_t)m * n * poly;
+    Group& fg = fwdg[{lgN, P * 16 + (r + 29) / 30}];  // one class per product
+    fg.P = P;
+    fg.lgN = lgN;
+    if (r > fg.max_r) fg.max_r = r;
     for (int side = 0; side < 2; ++side) {
       const auto& ents = side ? ps.b : ps.a;
       const uint64_t base = side ? pd.b_res : pd.a_res;
@@ -533,11 +567,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
         fd.P = (uint16_t)P;
         uint64_t nc = ((uint64_t)nl * 64 + r - 1) / r;
         fd.ncoef = (uint32_t)(nc < N ? nc : N);
-        auto& g = fwdg[{lgN, P * 16 + (r + 29) / 30}];
-        g.P = P;
-        g.lgN = lgN;
-        if (r > g.max_r) g.max_r = r;
-        g.idx.push_back((uint32_t)fwd_.size());
+        fg.idx.push_back((uint32_t)fwd_.size());
         fwd_.push_back(fd);
       }
     }
@@ -561,6 +591,15 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
         (use_tc ? tc_items_ : items_).push_back(it);
       }
     const uint64_t ncoef_c = (uint64_t)(prm.lenA + prm.lenB - 1);
+    Group& ig = invg[{lgN, P}];
+    ig.P = P;
+    ig.lgN = lgN;
+    Group& rg = recg[P];
+    rg.P = P;
+    {
+      auto it = rec_min_r.find(P);
+      if (it == rec_min_r.end() || r < it->second) rec_min_r[P] = r;
+    }
     for (int e = 0; e < m * n; ++e) {
       InvDesc id;
       id.res_off = pd.c_res + (uint64_t)e * poly;
@@ -579,15 +618,8 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       id.entry = (uint32_t)(first_out + e);
       const uint32_t ii = (uint32_t)inv_.size();
       inv_.push_back(id);
-      auto& g = invg[{lgN, P}];
-      g.P = P;
-      g.lgN = lgN;
-      g.idx.push_back(ii);
-      auto& rg = recg[P];
-      rg.P = P;
+      ig.idx.push_back(ii);
       rg.idx.push_back(ii);
-      auto it = rec_min_r.find(P);
-      if (it == rec_min_r.end() || r < it->second) rec_min_r[P] = r;
     }
   }
   if (out_entry > 0x7fffffffULL) return set_error(kErrTooLarge, "too many output entries");
@@ -641,10 +673,13 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   for (auto& kv : recg) {
     Group g = std::move(kv.second);
     g.max_r = (int)rec_min_r[g.P];  // narrowest r: sizes the CRT kernel's scratch
-    // longest entries first (the warp that gets one works longest)
-    std::stable_sort(g.idx.begin(), g.idx.end(), [&](uint32_t a, uint32_t b) {
-      return inv_[a].out_words > inv_[b].out_words;
-    });
+    // longest entries first (the warp that gets one works longest), ties in
+    // entry order: one sort of packed (longest-first key, index) integers
+    std::vector<uint64_t> keys(g.idx.size());
+    for (size_t i = 0; i < keys.size(); ++i)
+      keys[i] = ((uint64_t)(0xffffffffu - inv_[g.idx[i]].out_words) << 32) | g.idx[i];
+    std::sort(keys.begin(), keys.end());
+    for (size_t i = 0; i < keys.size(); ++i) g.idx[i] = (uint32_t)keys[i];
     rec_groups_.push_back(std::move(g));
   }
   for (auto* gs : {&fwd_groups_, &inv_groups_, &rec_groups_})
@@ -1075,12 +1110,16 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     return s;
   }
 
-  // chunks of consecutive whole products
+  // chunks of consecutive whole products; the first two are a quarter and
+  // a half of the others, so the first results start back sooner (the
+  // device->host copies are the pipeline's longest chain)
   std::vector<size_t> bounds{0};
   uint64_t acc = 0;
   for (size_t t = 0; t < specs.size(); ++t) {
     acc += limbs[t];
-    if (acc >= chunk && t + 1 < specs.size()) {
+    const size_t c = bounds.size() - 1;
+    const uint64_t target = c == 0 ? chunk / 4 : (c == 1 ? chunk / 2 : chunk);
+    if (acc >= target && t + 1 < specs.size()) {
       bounds.push_back(t + 1);
       acc = 0;
     }

@@ -247,6 +247,12 @@ bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* 
     if (budget < 3) continue;
     int r = budget / 2;
     if (r > kMaxCoeffBits) r = kMaxCoeffBits;
+    {
+      // lengths only grow as r shrinks, so no r above this one is feasible
+      const int64_t mn0 = ((a_bits < b_bits ? a_bits : b_bits) + r - 1) / r;
+      const int r1 = (budget - ceil_log2((uint64_t)mn0)) / 2;
+      if (r1 < r) r = r1;
+    }
     int64_t lenA = 0, lenB = 0;
     for (; r >= 1; --r) {
       lenA = (a_bits + r - 1) / r;
