@@ -406,37 +406,26 @@ __device__ __forceinline__ void fwd_last_pass(const uint32_t* s, uint32_t* out, 
   }
 }
 
-template <int D, bool TEAM>
-__global__ void __launch_bounds__(kFwdThreads, 3)
-k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
-       const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
-       uint32_t* __restrict__ res, const uint2* __restrict__ twf) {
-  extern __shared__ uint32_t sm[];
-  const CtaItem item = items[blockIdx.x];
-  const int lgN = item.lgN;
-  const int P = item.P;
+// The body of k_fwd2.  HZ: every polynomial of the CTA has at most N/2
+// coefficients (the usual case: both factors of a product fit in N
+// together), so the first pass's upper four points are zero: their digits
+// and residues are skipped and stage 0 only copies.
+template <int D, bool TEAM, bool HZ>
+__device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, bool valid, int lgN, int P,
+                                         int tt, int TS, const uint64_t* __restrict__ limbs,
+                                         uint32_t* __restrict__ res,
+                                         const uint2* __restrict__ twf) {
   const int N = 1 << lgN;
-  const int TS = TEAM ? (N >> 3) : kFwdThreads;  // threads per entry
-  const int team = TEAM ? (int)threadIdx.x / TS : 0;
-  const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
-  const bool valid = team < (int)item.count;
-  uint32_t* s = sm + team * (N + (N >> 5));
-  FwdDesc d;
-  d.limb_off = 0;
-  d.res_off = 0;
-  d.size = 0;
-  d.r = 1;
-  d.ncoef = 0;
-  if (valid) d = descs[idx[item.first + team]];
   const uint64_t nw = 2ull * (uint64_t)(d.size < 0 ? -d.size : d.size);
   const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
   const bool neg = d.size < 0;
   const int ng0 = N >> 3;  // groups (and the point stride) of the first pass
+  constexpr int QN = HZ ? 4 : 8;  // points of a first-pass group that can be nonzero
 
-  uint32_t dg[8][D];
+  uint32_t dg[QN][D];
   if (TEAM) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < QN; ++q) {
       const int x = q * ng0 + tt;
       coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
     }
@@ -448,13 +437,18 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
     for (int g = tt; g < ng0; g += TS) {
       uint32_t a[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < QN; ++q) {
         const int x = q * ng0 + g;
         if (!TEAM)
           coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
         a[q] = digits_residue<D>(dg[q], j, neg);
       }
-      fwd_group<3>(a, 0, 0, tw, p);
+      if (HZ) {
+        fwd_stage0_upper_zero<3>(a, p);
+        fwd_group<3, 1>(a, 0, 0, tw, p);
+      } else {
+        fwd_group<3>(a, 0, 0, tw, p);
+      }
       if (lgN == 3) {  // the only pass: eight consecutive points, straight out
         if (valid) store_points<3>(out, a, p);
       } else {
@@ -478,6 +472,35 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
     }
     __syncthreads();  // before the next prime's first pass overwrites s
   }
+}
+
+template <int D, bool TEAM>
+__global__ void __launch_bounds__(kFwdThreads, 3)
+k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
+       const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
+       uint32_t* __restrict__ res, const uint2* __restrict__ twf) {
+  extern __shared__ uint32_t sm[];
+  const CtaItem item = items[blockIdx.x];
+  const int lgN = item.lgN;
+  const int P = item.P;
+  const int N = 1 << lgN;
+  const int TS = TEAM ? (N >> 3) : kFwdThreads;  // threads per entry
+  const int team = TEAM ? (int)threadIdx.x / TS : 0;
+  const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
+  const bool valid = team < (int)item.count;
+  uint32_t* s = sm + team * (N + (N >> 5));
+  FwdDesc d;
+  d.limb_off = 0;
+  d.res_off = 0;
+  d.size = 0;
+  d.r = 1;
+  d.ncoef = 0;
+  if (valid) d = descs[idx[item.first + team]];
+  // one variant for the whole CTA (its barriers must be the same code)
+  if (__syncthreads_and(d.ncoef <= (uint32_t)(N >> 1)))
+    fwd_body<D, TEAM, true>(d, s, valid, lgN, P, tt, TS, limbs, res, twf);
+  else
+    fwd_body<D, TEAM, false>(d, s, valid, lgN, P, tt, TS, limbs, res, twf);
 }
 
 // Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.

@@ -38,12 +38,12 @@ __device__ __forceinline__ uint32_t reduce_2p(uint32_t x, uint32_t p2) {
 
 // Forward: L stages starting at s0 on the 2^L registers a[] of one group.
 // hi is the group's high index; twiddles from tw (the prime's table).
-template <int L>
+template <int L, int LSTART = 0>
 __device__ __forceinline__ void fwd_group(uint32_t (&a)[1 << L], int s0, int hi,
                                           const uint2* __restrict__ tw, uint32_t p) {
   const uint32_t p2 = 2 * p;
 #pragma unroll
-  for (int l = 0; l < L; ++l) {
+  for (int l = LSTART; l < L; ++l) {
     const int span = 1 << (L - 1 - l);
     const int m = 1 << (s0 + l);
 #pragma unroll
@@ -56,6 +56,20 @@ __device__ __forceinline__ void fwd_group(uint32_t (&a)[1 << L], int s0, int hi,
       a[q] = U + V;
       a[q + span] = U - V + p2;
     }
+  }
+}
+
+// First forward stage of a group whose upper half (points a[2^(L-1) ..])
+// is zero: every butterfly's product is 0, so it only copies -- the same
+// values the general butterfly gives (U and U + 2p).
+template <int L>
+__device__ __forceinline__ void fwd_stage0_upper_zero(uint32_t (&a)[1 << L], uint32_t p) {
+  const uint32_t p2 = 2 * p;
+#pragma unroll
+  for (int q = 0; q < (1 << (L - 1)); ++q) {
+    const uint32_t U = reduce_2p(a[q], p2);
+    a[q] = U;
+    a[q + (1 << (L - 1))] = U + p2;
   }
 }
 
