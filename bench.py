@@ -414,11 +414,19 @@ def main():
         names = ["split_fwd_ntt", "contract", "inv_ntt", "crt_recompose"]
         dom = int(np.argmax(stage_ms))
         if dom == 0:
-            alg, t_ms, kern = b1, stage_ms[0], "k_split_fwd"
+            alg, t_ms, kern, stage = b1, stage_ms[0], "k_fwd2 (split + forward NTT launches)", "fwd"
         elif dom == 1:
-            alg, t_ms, kern = b2, stage_ms[1], "k_contract"
+            alg, t_ms, kern, stage = b2, stage_ms[1], "k_contract", "contract"
         else:
-            alg, t_ms, kern = b3, stage_ms[2] + stage_ms[3], "k_inv_ntt+k_crt_recompose"
+            alg, t_ms, kern, stage = (b3, stage_ms[2] + stage_ms[3], "k_inv2+k_crt_warp",
+                                      "inv_crt")
+        # DRAM bytes per step of the stage on the 4096-product batch: ncu
+        # (dram__bytes_read.sum + dram__bytes_write.sum) on the 512-product
+        # step, scaled by the batch's residue points (x7.81 forward, x7.50
+        # contraction); profiles/ has the captures
+        traffic = None
+        if args.workload == "config3" and args.count == 4096:
+            traffic = {"fwd": 19.5e9, "contract": 32.9e9}.get(stage)
         peaks = load_peaks()
         per_launch_s = (t_ms / 1000.0) / max(1, timed)
         achieved = alg / per_launch_s / 1e9
@@ -456,8 +464,12 @@ def main():
                                    for n, t in zip(names, stage_ms)},
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved,
                          "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
-                         "peak_source": peaks[1], "traffic": None,
-                         "alg_bytes_per_step": alg},
+                         "peak_source": peaks[1], "traffic": traffic,
+                         "traffic_note": "DRAM bytes per step (ncu, 512-product step scaled)"
+                         if traffic else None,
+                         "alg_bytes_per_step": alg,
+                         "alg_note": "3-pass byte model at the reference's parameters "
+                                     "(4 primes, u64 residues)"},
             "cpu_baseline": cpu,
             "clocks": clk,
             "verified": verified,
