@@ -251,8 +251,9 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
                                    const int64_t *c_caps, int32_t *d_c_sizes, void *stream);
 
 /* ---- continuous-batching server (no counterpart in the reference) ----
-   A scheduler thread keeps up to `slots` batches in flight, each on its own
-   CUDA stream.  Whenever a slot is free it admits queued requests in arrival
+   Up to `slots` batches are in flight, each slot with its own host thread,
+   CUDA stream and workspace.  Whenever a slot is free it admits queued
+   requests in arrival
    order into one batch while their estimated device footprint fits what the
    in-flight batches leave of `budget_bytes` (0: three quarters of the free
    device memory), with at most `max_batch` products per batch (0: no

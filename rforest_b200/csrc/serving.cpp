@@ -1,17 +1,16 @@
 // Continuous-batching request server (mpzmm_server_* in include/mpzmm_b200.h).
 //
-// Callers submit single products from any thread; a scheduler thread owns the
-// GPU work.  It keeps up to `slots` batches in flight, each on its own CUDA
-// stream with its own grow-only workspace.  Whenever a slot is free it
-// admits queued requests in arrival order into a new batch while their
-// estimated device footprint fits what the in-flight batches leave of the
-// device-memory budget, plans the batch (one launch per stage), copies its
-// inputs, launches it and records an event; batches finishing are copied
-// back and their requests completed.  So requests that arrive while others
-// are on the GPU join the next batch as soon as a slot and memory are free,
-// and batches on different slots overlap on the device.  No call inside the
-// scheduler waits on the device except the copy-back of a batch whose event
-// has already completed.
+// Callers submit single products from any thread.  The server keeps up to
+// `slots` batches in flight; each slot has its own host thread, CUDA stream
+// and grow-only workspace.  A free slot admits queued requests in arrival
+// order into a new batch while their estimated device footprint fits what
+// the batches in flight leave of the device-memory budget, plans the batch
+// (one launch per stage), copies its inputs, launches it, waits for it on
+// its own stream and copies the results back.  So requests that arrive
+// while others are on the GPU join the next batch as soon as a slot and
+// memory are free, batches on different slots overlap on the device, and
+// the host work of one slot (planning, copies, a workspace growing) never
+// holds up the others.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -46,11 +45,8 @@ struct Ticket {
 
 struct Slot {
   cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
   Workspace ws;
-  std::unique_ptr<Plan> plan;
-  std::vector<std::shared_ptr<Ticket>> tickets;
-  int64_t bytes = 0;
+  std::thread thread;
   bool busy = false;
 };
 
@@ -59,19 +55,19 @@ struct Slot {
 struct mpzmm_server {
   int64_t budget = 0;
   int max_batch = 0;
+  int device = 0;
   std::vector<std::unique_ptr<Slot>> slots;
   std::mutex mu;
-  std::condition_variable cv_work;  // scheduler wakes up
+  std::condition_variable cv_work;  // slots wake up: new request, freed budget, stop
   std::condition_variable cv_done;  // waiters wake up
   std::deque<std::shared_ptr<Ticket>> queue;
   std::unordered_map<uint64_t, std::shared_ptr<Ticket>> tickets;
   uint64_t next_id = 1;
   bool stop = false;
-  std::thread thread;
   int64_t in_flight_bytes = 0;
   int64_t stat_batches = 0, stat_products = 0, stat_max_in_flight = 0;
-  // scheduler-thread time per phase (ns): plan build, input gather + copy,
-  // launches, result copy-back + scatter
+  // slot-thread time per phase, summed over slots (ns): plan build, input
+  // gather + copy, launches, wait + result copy-back + scatter
   int64_t ns_build = 0, ns_upload = 0, ns_launch = 0, ns_download = 0;
 
   void complete(const std::shared_ptr<Ticket>& t, int status, const std::string& err) {
@@ -80,121 +76,90 @@ struct mpzmm_server {
     t->t_done = now_ns();
   }
 
-  // Launches one admitted batch on a free slot (scheduler thread, lock not held).
-  void launch(Slot& s, std::vector<std::shared_ptr<Ticket>> batch, int64_t bytes) {
+  // Admits queued requests for a free slot (lock held): FIFO, at most
+  // max_batch, while the estimated footprint fits the free budget; a
+  // request larger than the free budget runs once the GPU is otherwise idle.
+  void admit(std::vector<std::shared_ptr<Ticket>>& batch, int64_t& bytes) {
+    int busy_slots = 0;
+    for (auto& o : slots) busy_slots += o->busy ? 1 : 0;
+    while (!queue.empty() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
+      const auto& t = queue.front();
+      const bool fits = in_flight_bytes + bytes + t->bytes <= budget;
+      const bool alone = batch.empty() && busy_slots == 0 && in_flight_bytes == 0 &&
+                         t->bytes <= budget;
+      if (!fits && !alone) break;
+      bytes += t->bytes;
+      batch.push_back(t);
+      queue.pop_front();
+      if (!fits) break;
+    }
+  }
+
+  // One batch on a slot (slot thread, lock not held): returns its status.
+  int run_batch_on(Slot& s, std::vector<std::shared_ptr<Ticket>>& batch, std::string* err) {
     std::vector<ProductSpec> specs;
     specs.reserve(batch.size());
     for (auto& t : batch) specs.push_back(t->spec);
-    s.plan.reset(new Plan);
+    Plan plan;
     const int64_t a0 = now_ns();
-    int st = s.plan->build(std::move(specs), &s.ws);
+    int st = plan.build(std::move(specs), &s.ws);
     const int64_t a1 = now_ns();
-    if (!st) st = s.plan->upload(s.stream);
+    if (!st) st = plan.upload(s.stream);
     const int64_t a2 = now_ns();
-    if (!st) st = s.plan->execute(s.stream);
-    if (!st) {
-      const cudaError_t e = cudaEventRecord(s.done, s.stream);
-      if (e != cudaSuccess) st = set_error(kErrCuda, cudaGetErrorString(e));
+    if (!st) st = plan.execute(s.stream);
+    const int64_t a3 = now_ns();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (auto& t : batch) t->t_start = a3;
     }
-    const int64_t t0 = now_ns();
+    if (!st) st = plan.download(s.stream);
+    const int64_t a4 = now_ns();
+    if (st) {
+      *err = last_error();
+      cudaStreamSynchronize(s.stream);  // whatever was queued
+    }
+    std::lock_guard<std::mutex> lk(mu);
     ns_build += a1 - a0;
     ns_upload += a2 - a1;
-    ns_launch += t0 - a2;
-    std::lock_guard<std::mutex> lk(mu);
-    for (auto& t : batch) t->t_start = t0;
-    if (st) {
-      const std::string err = last_error();
-      for (auto& t : batch) complete(t, st, err);
-      in_flight_bytes -= bytes;
-      s.plan.reset();
-      s.ws.release_device();
-      cv_done.notify_all();
-      return;
-    }
-    s.tickets = std::move(batch);
-    s.bytes = bytes;
-    s.busy = true;
-    ++stat_batches;
+    ns_launch += a3 - a2;
+    ns_download += a4 - a3;
+    return st;
   }
 
-  // Copies back a finished batch and completes its tickets.
-  void finish(Slot& s) {
-    const int64_t d0 = now_ns();
-    const int st = s.plan->download(s.stream);
-    ns_download += now_ns() - d0;
-    const std::string err = st ? last_error() : std::string();
-    s.plan.reset();
-    // workspaces are grow-only (re-growing per batch costs far more than the
-    // batch); one that has grown past its share of the budget is released
-    if (s.ws.device_bytes > budget / (int64_t)slots.size()) s.ws.release_device();
-    std::lock_guard<std::mutex> lk(mu);
-    for (auto& t : s.tickets) complete(t, st, err);
-    stat_products += (int64_t)s.tickets.size();
-    in_flight_bytes -= s.bytes;
-    s.tickets.clear();
-    s.bytes = 0;
-    s.busy = false;
-    cv_done.notify_all();
-  }
-
-  void run() {
-    cudaSetDevice(context().device);
+  void slot_loop(Slot& s) {
+    cudaSetDevice(device);
     for (;;) {
-      bool progressed = false;
-      // completions
-      for (auto& sp : slots) {
-        Slot& s = *sp;
-        if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
-          finish(s);
-          progressed = true;
+      std::vector<std::shared_ptr<Ticket>> batch;
+      int64_t bytes = 0;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+          admit(batch, bytes);
+          if (!batch.empty()) break;
+          if (stop && queue.empty()) return;
+          cv_work.wait(lk);
         }
+        s.busy = true;
+        in_flight_bytes += bytes;
+        ++stat_batches;
+        int in_flight = 0;
+        for (auto& o : slots) in_flight += o->busy ? 1 : 0;
+        if (in_flight > stat_max_in_flight) stat_max_in_flight = in_flight;
       }
-      // admissions
-      for (auto& sp : slots) {
-        Slot& s = *sp;
-        if (s.busy) continue;
-        std::vector<std::shared_ptr<Ticket>> batch;
-        int64_t bytes = 0;
-        {
-          std::lock_guard<std::mutex> lk(mu);
-          int busy_slots = 0;
-          for (auto& o : slots) busy_slots += o->busy ? 1 : 0;
-          while (!queue.empty() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
-            const auto& t = queue.front();
-            const bool fits = in_flight_bytes + bytes + t->bytes <= budget;
-            // a request larger than the free budget still runs once the GPU
-            // is otherwise idle (admitting alone), as long as it fits at all
-            const bool alone = batch.empty() && busy_slots == 0 && in_flight_bytes == 0 &&
-                               t->bytes <= budget;
-            if (!fits && !alone) break;
-            bytes += t->bytes;
-            batch.push_back(t);
-            queue.pop_front();
-            if (!fits) break;
-          }
-          if (!batch.empty()) {
-            in_flight_bytes += bytes;
-            int in_flight = 1;
-            for (auto& o : slots) in_flight += o->busy ? 1 : 0;
-            if (in_flight > stat_max_in_flight) stat_max_in_flight = in_flight;
-          }
-        }
-        if (!batch.empty()) {
-          launch(s, std::move(batch), bytes);
-          progressed = true;
-        }
+      std::string err;
+      const int st = run_batch_on(s, batch, &err);
+      // workspaces are grow-only (re-growing per batch costs far more than the
+      // batch); one that has grown past its share of the budget is released
+      if (st || s.ws.device_bytes > budget / (int64_t)slots.size()) s.ws.release_device();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& t : batch) complete(t, st, err);
+        stat_products += (int64_t)batch.size();
+        in_flight_bytes -= bytes;
+        s.busy = false;
       }
-      std::unique_lock<std::mutex> lk(mu);
-      bool any_busy = false;
-      for (auto& sp : slots) any_busy |= sp->busy;
-      if (stop && queue.empty() && !any_busy) break;
-      if (!progressed) {
-        if (any_busy)
-          cv_work.wait_for(lk, std::chrono::microseconds(20));
-        else
-          cv_work.wait_for(lk, std::chrono::milliseconds(5),
-                           [&] { return stop || !queue.empty(); });
-      }
+      cv_done.notify_all();
+      cv_work.notify_all();  // freed budget: another slot may admit now
     }
   }
 };
@@ -216,15 +181,21 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
   }
   s->budget = budget_bytes;
   s->max_batch = max_batch;
+  s->device = context().device;
   for (int i = 0; i < slots; ++i) {
     std::unique_ptr<Slot> sl(new Slot);
     cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming);
-    if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+      for (auto& o : s->slots) cudaStreamDestroy(o->stream);
+      return set_error(kErrCuda, cudaGetErrorString(e));
+    }
     s->slots.push_back(std::move(sl));
   }
   mpzmm_server* raw = s.get();
-  s->thread = std::thread([raw] { raw->run(); });
+  for (auto& sl : s->slots) {
+    Slot* sp = sl.get();
+    sl->thread = std::thread([raw, sp] { raw->slot_loop(*sp); });
+  }
   *out = s.release();
   return kOk;
 }
@@ -261,7 +232,7 @@ int mpzmm_server_submit(mpzmm_server* s, const mpzmm_product* req, uint64_t* tic
     s->tickets[t->id] = t;
     s->queue.push_back(t);
   }
-  s->cv_work.notify_one();
+  s->cv_work.notify_all();
   *ticket = t->id;
   return kOk;
 }
@@ -340,11 +311,11 @@ void mpzmm_server_destroy(mpzmm_server* s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
-  if (s->thread.joinable()) s->thread.join();  // drains queued and in-flight work
+  for (auto& sl : s->slots)  // the slots drain queued and in-flight work first
+    if (sl->thread.joinable()) sl->thread.join();
   for (auto& sl : s->slots) {
     cudaStreamSynchronize(sl->stream);
     sl->ws.release();
-    cudaEventDestroy(sl->done);
     cudaStreamDestroy(sl->stream);
   }
   delete s;
