@@ -185,6 +185,26 @@ typedef struct mpzmm_product {
    mpzmm_output_limbs(k, exact operand bit lengths).  Synchronous. */
 MPZMM_API int mpzmm_matmul_batch(int count, const mpzmm_product *products, void *stream);
 
+/* ---- device-resident chains (no counterpart in the reference) ----
+   M = X_0 X_1 ... X_{count-1} left to right (X_0 r x c_0, X_i c_{i-1} x c_i,
+   packed vectors as above), the running product kept in device memory
+   between steps: step i copies step i-1's result limbs on the device and
+   reads its signs and sizes there, so nothing crosses the host link but the
+   X_i and the final result.  Each step is planned for a bound of the
+   running product (64 x the previous step's output limbs), so every step is
+   exact; mpzmm_chain_output_limbs gives the final entries' capacity (-1 for
+   a malformed chain).  Synchronous. */
+typedef struct mpzmm_matrix {
+  int rows, cols;
+  const uint64_t *limbs;
+  const int64_t *offs;
+  const int32_t *sizes;
+} mpzmm_matrix;
+MPZMM_API int64_t mpzmm_chain_output_limbs(int count, const mpzmm_matrix *mats);
+MPZMM_API int mpzmm_chain(int count, const mpzmm_matrix *mats, uint64_t *c_limbs,
+                          const int64_t *c_offs, const int64_t *c_caps, int32_t *c_sizes,
+                          void *stream);
+
 /* ---- device-resident plans (build once, run many times) ---- */
 typedef struct mpzmm_plan mpzmm_plan;
 

@@ -38,6 +38,14 @@ class Product(C.Structure):
     ]
 
 
+class Matrix(C.Structure):
+    """struct mpzmm_matrix."""
+    _fields_ = [
+        ("rows", C.c_int), ("cols", C.c_int),
+        ("limbs", u64p), ("offs", i64p), ("sizes", i32p),
+    ]
+
+
 class MpzmmError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"mpzmm status {status}: {message}")
@@ -105,6 +113,8 @@ def lib():
         "mpzmm_host_register": (C.c_int, [vp, C.c_size_t]),
         "mpzmm_host_unregister": (C.c_int, [vp]),
         "mpzmm_batch_stats": (C.c_int, [i64p, i64p, i64p]),
+        "mpzmm_chain_output_limbs": (C.c_int64, [C.c_int, C.POINTER(Matrix)]),
+        "mpzmm_chain": (C.c_int, [C.c_int, C.POINTER(Matrix), u64p, i64p, i64p, i32p, vp]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

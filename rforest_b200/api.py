@@ -236,6 +236,36 @@ def matmul_batch(products: Sequence[ProductIn], stream=None) -> List[Packed]:
     return Batch(products).run(stream)
 
 
+def chain(mats: Sequence[Tuple[int, int, Packed]], stream=None) -> Packed:
+    """M = X_0 X_1 ... X_{n-1} (each (rows, cols, packed row-major entries)),
+    the running product kept in device memory between the steps."""
+    keep = []
+    arr = (_lib.Matrix * len(mats))()
+    for i, (rows, cols, X) in enumerate(mats):
+        if len(X) != rows * cols:
+            raise ValueError("entry count does not match the dimensions")
+        limbs = np.ascontiguousarray(X.limbs, dtype=np.uint64)
+        if limbs.size == 0:
+            limbs = np.zeros(1, np.uint64)
+        offs = np.ascontiguousarray(X.offs, dtype=np.int64)
+        sizes = np.ascontiguousarray(X.sizes, dtype=np.int32)
+        keep += [limbs, offs, sizes]
+        arr[i] = _lib.Matrix(rows, cols, _ptr(limbs, _lib.u64p), _ptr(offs, _lib.i64p),
+                             _ptr(sizes, _lib.i32p))
+    cap = int(_lib.lib().mpzmm_chain_output_limbs(len(mats), arr))
+    if cap < 0:
+        _lib.check(_lib.MPZMM_ERR_ARG)
+    m, n = mats[0][0], mats[-1][1]
+    cl = np.zeros(max(m * n * cap, 1), dtype=np.uint64)
+    co = np.arange(m * n, dtype=np.int64) * cap
+    caps = np.full(m * n, cap, dtype=np.int64)
+    csz = np.zeros(m * n, dtype=np.int32)
+    _lib.check(_lib.lib().mpzmm_chain(len(mats), arr, _ptr(cl, _lib.u64p), _ptr(co, _lib.i64p),
+                                      _ptr(caps, _lib.i64p), _ptr(csz, _lib.i32p),
+                                      _stream_arg(stream)))
+    return Packed(cl, co, csz)
+
+
 class Plan:
     """A device-resident batch: inputs uploaded once, executed many times."""
 

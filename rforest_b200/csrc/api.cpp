@@ -277,6 +277,103 @@ int mpzmm_matmul_batch(int count, const mpzmm_product* products, void* stream) {
   return run_once(std::move(specs), stream);
 }
 
+namespace {
+int64_t matrix_max_bits(const mpzmm_matrix& x) {
+  int64_t bits = 0;
+  for (int64_t e = 0; e < (int64_t)x.rows * x.cols; ++e) {
+    const int32_t s = x.sizes[e];
+    if (!s) continue;
+    const EntryRef r{x.limbs + x.offs[e], s};
+    const int64_t b = bit_length(r);
+    if (b > bits) bits = b;
+  }
+  return bits;
+}
+
+int check_chain(int count, const mpzmm_matrix* mats) {
+  if (count < 2 || !mats) return set_error(kErrArg, "a chain needs at least two matrices");
+  for (int i = 0; i < count; ++i) {
+    const mpzmm_matrix& x = mats[i];
+    if (x.rows < 1 || x.cols < 1) return set_error(kErrArg, "chain matrix without entries");
+    if (!x.offs || !x.sizes || !x.limbs) return set_error(kErrArg, "null array");
+    if (i > 0 && x.rows != mats[i - 1].cols)
+      return set_error(kErrArg, "chain matrix " + std::to_string(i) + " has " +
+                                    std::to_string(x.rows) + " rows, expected " +
+                                    std::to_string(mats[i - 1].cols));
+  }
+  return kOk;
+}
+
+// Output limb bound of every chain step (the planner's own: exact bits for
+// the host operands, 64 x the previous bound for the running product).
+int chain_limbs(int count, const mpzmm_matrix* mats, std::vector<int64_t>* limbs, bool* zero) {
+  *zero = false;
+  std::vector<int64_t> bits((size_t)count);
+  for (int i = 0; i < count; ++i) {
+    bits[i] = matrix_max_bits(mats[i]);
+    if (!bits[i]) *zero = true;
+  }
+  limbs->assign((size_t)count - 1, 1);
+  if (*zero) return kOk;
+  int64_t a_bits = bits[0];
+  for (int i = 1; i < count; ++i) {
+    (*limbs)[i - 1] = output_limbs(mats[i].rows, a_bits, bits[i]);
+    a_bits = 64 * (*limbs)[i - 1];
+  }
+  return kOk;
+}
+}  // namespace
+
+int64_t mpzmm_chain_output_limbs(int count, const mpzmm_matrix* mats) {
+  if (check_chain(count, mats)) return -1;
+  std::vector<int64_t> lim;
+  bool zero;
+  chain_limbs(count, mats, &lim, &zero);
+  return zero ? 1 : lim.back();
+}
+
+int mpzmm_chain(int count, const mpzmm_matrix* mats, uint64_t* c_limbs, const int64_t* c_offs,
+                const int64_t* c_caps, int32_t* c_sizes, void* stream) {
+  int st = check_chain(count, mats);
+  if (st) return st;
+  const int m = mats[0].rows, n = mats[count - 1].cols;
+  if (!c_limbs || !c_offs || !c_caps || !c_sizes) return set_error(kErrArg, "null output array");
+  if ((st = ensure_setup(-1))) return st;
+  std::vector<int64_t> lim;
+  bool zero;
+  chain_limbs(count, mats, &lim, &zero);
+  if (zero) {  // a zero factor: the product is zero
+    for (int64_t e = 0; e < (int64_t)m * n; ++e) c_sizes[e] = 0;
+    return kOk;
+  }
+  auto host_entries = [](const mpzmm_matrix& x, std::vector<EntryRef>* v) {
+    v->resize((size_t)x.rows * x.cols);
+    for (size_t e = 0; e < v->size(); ++e) {
+      const int32_t s = x.sizes[e];
+      (*v)[e] = EntryRef{s ? x.limbs + x.offs[e] : nullptr, s};
+    }
+  };
+  std::vector<ProductSpec> steps((size_t)count - 1);
+  for (int i = 1; i < count; ++i) {
+    ProductSpec& ps = steps[(size_t)i - 1];
+    ps.m = m;
+    ps.k = mats[i].rows;
+    ps.n = mats[i].cols;
+    if (i == 1) {
+      host_entries(mats[0], &ps.a);
+    } else {
+      ps.a.assign((size_t)ps.m * ps.k, EntryRef{nullptr, 0});  // on the device
+    }
+    host_entries(mats[i], &ps.b);
+    ps.c.resize((size_t)ps.m * ps.n);
+    for (size_t e = 0; e < ps.c.size(); ++e)
+      ps.c[e] = i + 1 == count ? OutRef{c_limbs + c_offs[e], c_caps[e], c_sizes + e, nullptr}
+                               : OutRef{nullptr, 0, nullptr, nullptr};
+  }
+  std::lock_guard<std::mutex> lk(workspace_mutex());
+  return run_chain(std::move(steps), pick_stream(stream));
+}
+
 int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* products,
                       void* stream) {
   if (!plan) return set_error(kErrArg, "null plan pointer");

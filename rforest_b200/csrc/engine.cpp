@@ -37,6 +37,8 @@ int cuda_status(cudaError_t e, const char* what) {
     if (_e != cudaSuccess) return cuda_fail(_e, what); \
   } while (0)
 
+}  // namespace
+
 int64_t bit_length(const EntryRef& e) {
   int64_t i = (e.size < 0 ? -(int64_t)e.size : e.size) - 1;
   // a non-normalised top limb of zero is tolerated: scan down
@@ -44,6 +46,8 @@ int64_t bit_length(const EntryRef& e) {
   if (i < 0) return 0;
   return 64 * i + (64 - __builtin_clzll(e.d[i]));
 }
+
+namespace {
 
 }  // namespace
 
@@ -417,6 +421,10 @@ static int plan_product(const ProductSpec& ps, Params* prm, std::string* msg) {
   for (int side = 0; side < 2; ++side) {
     const auto& ents = side ? ps.b : ps.a;
     int64_t& bits = side ? b_bits : a_bits;
+    if (!side && ps.dev_a) {  // values on the device: plan for the bound
+      bits = 64 * ps.dev_a->cap_limbs;
+      continue;
+    }
     // only the longest entries can hold the largest bit length: read their
     // top limbs (each read of a caller's limb is a likely cache miss, so
     // they are prefetched together first), and scan everything only when
@@ -488,6 +496,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     const int m = ps.m, k = ps.k, n = ps.n;
     const Params prm = params_[t];
     const uint64_t first_out = out_entry;
+    prod_first_out_.push_back((size_t)first_out);
     for (auto& c : ps.c) outs_.push_back(c);
     out_entry += ps.c.size();
     if (prm.P == 0 || m == 0 || n == 0) {
@@ -527,6 +536,30 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     for (int side = 0; side < 2; ++side) {
       const auto& ents = side ? ps.b : ps.a;
       const uint64_t base = side ? pd.b_res : pd.a_res;
+      if (!side && ps.dev_a) {
+        // the operand's limbs are copied on the device as one span (256-byte
+        // aligned); its sizes are written into the descriptors on the device
+        const DeviceOperand& da = *ps.dev_a;
+        n_limbs_ = (n_limbs_ + 31) & ~(uint64_t)31;
+        const uint64_t span0 = n_limbs_;
+        dev_runs_.push_back(DevRun{da.limbs, span0, da.span_limbs});
+        dev_fixes_.push_back(DevFix{da.sizes, (uint32_t)fwd_.size(), (uint32_t)ents.size()});
+        n_limbs_ += da.span_limbs;
+        host_end = nullptr;
+        for (size_t e = 0; e < ents.size(); ++e) {
+          FwdDesc fd;
+          fd.limb_off = span0 + (uint64_t)da.offs[e];
+          fd.res_off = base + e * poly;
+          fd.size = (int32_t)da.cap_limbs;  // replaced on the device
+          fd.r = (uint32_t)r;
+          fd.lgN = (uint16_t)lgN;
+          fd.P = (uint16_t)P;
+          fd.ncoef = (uint32_t)N;  // replaced on the device
+          fg.idx.push_back((uint32_t)fwd_.size());
+          fwd_.push_back(fd);
+        }
+        continue;
+      }
       for (size_t e = 0; e < ents.size(); ++e) {
         FwdDesc fd;
         const int64_t nl = ents[e].size < 0 ? -(int64_t)ents[e].size : ents[e].size;
@@ -757,7 +790,7 @@ void Plan::plan_transfers() {
     const size_t cnt = prods_[t].c.size();
     const size_t first = e0;
     e0 += cnt;
-    if (!cnt || zero_prod_[t]) continue;
+    if (!cnt || zero_prod_[t] || prods_[t].device_only) continue;
     const int64_t lim = out_limbs_[first];
     const uint64_t width = 2 * (uint64_t)lim;  // words per entry on the device
     const uint64_t dev = (uint64_t)out_word_off_[first];
@@ -819,6 +852,14 @@ int Plan::upload(cudaStream_t st) {
     CU(cudaMemcpyAsync(ws_->d_desc, ws_->h_desc, desc_bytes_, cudaMemcpyHostToDevice, st),
        "H2D descriptors");
   CU(cudaMemsetAsync(ws_->d_status, 0, sizeof(int), st), "clear status");
+  // operands already on the device: copy their limbs, then write their
+  // sizes into the forward descriptors
+  for (const DevRun& r : dev_runs_)
+    if (r.n)
+      CU(cudaMemcpyAsync(ws_->d_limbs + r.dst, r.src, r.n * 8, cudaMemcpyDeviceToDevice, st),
+         "D2D limbs");
+  for (const DevFix& f : dev_fixes_)
+    CU(launch_fix_sizes(d_fwd_ + f.first_fwd, (int)f.count, f.sizes, st), "size fix-up launch");
   // straight copies first, so the DMA runs while the staged runs are gathered
   for (const Run& r : in_runs_)
     if (r.direct)
@@ -1027,6 +1068,21 @@ int Plan::download_finish(cudaStream_t st, cudaEvent_t done) {
     }
   });
   return status;
+}
+
+DeviceOperand Plan::device_output(size_t product) const {
+  DeviceOperand o;
+  const size_t first = prod_first_out_[product];
+  const size_t cnt = prods_[product].c.size();
+  if (!cnt || zero_prod_[product]) return o;
+  const uint64_t w0 = (uint64_t)out_word_off_[first];  // even: whole limbs
+  o.limbs = reinterpret_cast<const uint64_t*>(ws_->d_out + w0);
+  o.sizes = ws_->d_sizes + first;
+  o.cap_limbs = out_limbs_[first];
+  o.offs.resize(cnt);
+  for (size_t e = 0; e < cnt; ++e) o.offs[e] = (out_word_off_[first + e] - (int64_t)w0) / 2;
+  o.span_limbs = (uint64_t)o.offs[cnt - 1] + (uint64_t)o.cap_limbs;
+  return o;
 }
 
 int Plan::download(cudaStream_t st) {
@@ -1253,6 +1309,37 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   ctx.batch_ns[2] = sub_ns[1];
   if (sub_status && (!status || status == kErrCapacity)) status = set_error(sub_status, sub_msg);
   return status;
+}
+
+int run_chain(std::vector<ProductSpec> steps, cudaStream_t st) {
+  Context& ctx = context();
+  if (steps.empty()) return kOk;
+  int s = ensure_pipeline(ctx);
+  if (s) return s;
+  // two workspaces in turn: step i reads step i-1's results (device to
+  // device) while step i+1 may already be planned into the other one, after
+  // the copies of the step that used it last have left its host buffers
+  std::unique_ptr<Plan> prev;
+  for (size_t i = 0; i < steps.size(); ++i) {
+    const int w = (int)(i & 1);
+    ProductSpec& ps = steps[i];
+    if (i > 0) {
+      const DeviceOperand o = prev->device_output(0);
+      if (!o.limbs) return set_error(kErrState, "chain step without device results");
+      ps.dev_a = std::make_shared<DeviceOperand>(o);
+    }
+    ps.device_only = i + 1 < steps.size();
+    CU(cudaEventSynchronize(ctx.pipe_ev_in[w]), "wait for a workspace's copies");
+    std::unique_ptr<Plan> cur(new Plan);
+    std::vector<ProductSpec> one;
+    one.push_back(std::move(ps));
+    if ((s = cur->build(std::move(one), ctx.pipe_ws[w]))) return s;
+    if ((s = cur->upload(st))) return s;
+    CU(cudaEventRecord(ctx.pipe_ev_in[w], st), "cudaEventRecord");
+    if ((s = cur->execute(st))) return s;
+    prev = std::move(cur);
+  }
+  return prev->download(st);
 }
 
 }  // namespace mpzmm

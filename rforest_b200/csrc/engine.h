@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -47,10 +48,28 @@ struct OutRef {
   void* mpz;         // mpz_ptr destination (mpz output) or nullptr
 };
 
+// An operand already in device memory (the output of an earlier plan):
+// entry e's limbs at limbs + offs[e] (at most cap_limbs of them, zero above
+// the value), its signed size at sizes[e]; the sizes are read on the device.
+struct DeviceOperand {
+  const uint64_t* limbs = nullptr;
+  const int32_t* sizes = nullptr;
+  std::vector<int64_t> offs;
+  int64_t cap_limbs = 0;
+  uint64_t span_limbs = 0;  // limbs from limbs[0] to the end of the last entry
+};
+
+// Bit length of an entry's magnitude (0 for zero).
+int64_t bit_length(const EntryRef& e);
+
 struct ProductSpec {
   int m = 0, k = 0, n = 0;
   std::vector<EntryRef> a, b;  // m*k and k*n entries, row-major
   std::vector<OutRef> c;       // m*n entries
+  // A in device memory instead of `a` (whose sizes are then ignored)
+  std::shared_ptr<DeviceOperand> dev_a;
+  // results stay on the device for a later plan (no host outputs)
+  bool device_only = false;
 };
 
 // Device and pinned host buffers of a plan.  Grow-only, so one workspace is
@@ -201,6 +220,9 @@ class Plan {
   }
   uint64_t direct_in_bytes() const { return direct_in_limbs_ * 8; }
   uint64_t direct_out_bytes() const { return direct_out_words_ * 4; }
+  // the results on the device (valid until the workspace is reused):
+  // product t's output entry e at output limb offset out_limb_offset(...)
+  DeviceOperand device_output(size_t product) const;
 
   int64_t launches_per_execute() const { return launches_; }
   // Stage timing with CUDA events recorded on the execute stream: stages are
@@ -252,6 +274,20 @@ class Plan {
     uint64_t rows, pitch;
   };
   std::vector<Run> in_runs_, out_runs_;
+  // device-resident operands: limb spans copied on the device, and the
+  // forward descriptors whose sizes come from device memory
+  struct DevRun {
+    const uint64_t* src;
+    uint64_t dst, n;
+  };
+  std::vector<DevRun> dev_runs_;
+  struct DevFix {
+    const int32_t* sizes;  // device array of the operand
+    uint32_t first_fwd;    // descriptors first_fwd .. + count - 1
+    uint32_t count;
+  };
+  std::vector<DevFix> dev_fixes_;
+  std::vector<size_t> prod_first_out_;  // first output entry of each product
   std::vector<int64_t> out_stage_;    // per output entry: staging word offset, -1 if direct
   uint64_t stage_limbs_ = 0, stage_out_words_ = 0;
   uint64_t direct_in_limbs_ = 0, direct_out_words_ = 0;
@@ -292,5 +328,11 @@ class Plan {
 // their results (two copy streams also keep the copy directions on
 // separate copy queues).  Returns when every result is written.
 int run_batch(std::vector<ProductSpec> specs, cudaStream_t st);
+
+// Chain of products, each step's A being the previous step's result kept in
+// device memory (steps[0] is an ordinary product; steps[i > 0] give B and
+// the dimensions, their `a` entries are placeholders); only the last step's
+// results are copied back to its outputs.  Returns when they are written.
+int run_chain(std::vector<ProductSpec> steps, cudaStream_t st);
 
 }  // namespace mpzmm

@@ -1003,6 +1003,30 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// Sizes of operands that live in device memory (results of an earlier plan):
+// the planner sized their transforms for a bound; the true signed size and
+// coefficient count go into the forward descriptors before the transforms.
+// ---------------------------------------------------------------------------
+__global__ void k_fix_sizes(FwdDesc* __restrict__ descs, int count,
+                            const int32_t* __restrict__ sizes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  FwdDesc d = descs[i];
+  const int32_t sz = sizes[i];
+  const uint64_t nl = (uint64_t)(sz < 0 ? -(int64_t)sz : sz);
+  const uint64_t nc = (nl * 64 + d.r - 1) / d.r;
+  const uint64_t N = (uint64_t)1 << d.lgN;
+  descs[i].size = sz;
+  descs[i].ncoef = (uint32_t)(nc < N ? nc : N);
+}
+
+cudaError_t launch_fix_sizes(FwdDesc* descs, int count, const int32_t* sizes, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  k_fix_sizes<<<(count + 255) / 256, 256, 0, st>>>(descs, count, sizes);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt) {

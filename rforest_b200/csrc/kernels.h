@@ -35,6 +35,9 @@ cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const Ct
 cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, int count,
                             uint32_t* res, cudaStream_t st);
 int contract_block_freqs();
+// writes the device-held signed sizes (and coefficient counts) of `count`
+// forward descriptors
+cudaError_t launch_fix_sizes(FwdDesc* descs, int count, const int32_t* sizes, cudaStream_t st);
 
 // Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
 // k <= 64, n <= 64; each work item covers `fb` consecutive frequencies.
