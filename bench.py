@@ -527,6 +527,22 @@ def compare_forms(api, torch, stream, triples, args):
         "value": len(sample) / dt, "unit": UNIT,
         "timing": f"wall clock, mpzmm_matmul per product with host buffers, first {len(sample)}"}
     api.set_contract_mode(0)
+    # config-2 chain (16 signed 8x8 matrices of 65536-bit entries, left to
+    # right): device-resident chain against one host round trip per step
+    from rforest_b200 import packed as PK, workloads as W
+    mats = W.config2_chain()
+    api.chain([(8, 8, X) for X in mats])  # warm the workspaces
+    t0 = time.perf_counter()
+    C = api.chain([(8, 8, X) for X in mats])
+    t_dev = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    M = mats[0]
+    for X in mats[1:]:
+        M = api.matmul(8, 8, 8, M, X).compact()
+    t_host = time.perf_counter() - t0
+    out["config2_chain"] = {"device_resident_ms": t_dev * 1e3, "host_round_trips_ms": t_host * 1e3,
+                            "same_result": PK.digest(C) == PK.digest(M),
+                            "timing": "wall clock, 15 products, inputs and result in host memory"}
     return out
 
 
