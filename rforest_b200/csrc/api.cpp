@@ -161,7 +161,11 @@ int mpzmm_autotune(void* stream, float* ms_out) {
         }
         ms[mode - 1] = best < 0.f ? 0.f : best;
       }
-      context().tc_pref[bk][bm] = ms[1] < ms[0] ? 1 : 0;
+      // tensor cores only with a clear margin: the probe is one product, and
+      // in a large batch the tensor-core kernel's per-block set-up weighs
+      // more than it does here (a near tie measured on one product turned
+      // into a 20x slower contraction of the 4096-product batch)
+      context().tc_pref[bk][bm] = ms[1] < 0.75f * ms[0] ? 1 : 0;
       if (ms_out) {
         ms_out[2 * (bk * 5 + bm)] = ms[0];
         ms_out[2 * (bk * 5 + bm) + 1] = ms[1];

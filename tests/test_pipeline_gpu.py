@@ -219,3 +219,34 @@ def test_pinned_inputs_with_gaps(gpu):
     finally:
         api.set_chunk_limbs(0)
         arena.close()
+
+
+def test_pipeline_edge_cases(small_chunks):
+    """Empty batch; zero products, 1 x 1 products and empty-sized entries
+    mixed into a pipelined batch (chunks that are partly or wholly zero)."""
+    assert api.matmul_batch([]) == []
+    rng = random.Random(67)
+    prods = []
+    for t in range(60):
+        kind = t % 5
+        m, k, n = rng.randrange(1, 5), rng.randrange(1, 5), rng.randrange(1, 5)
+        if kind == 0:    # A is all zero
+            A = PK.from_ints([0] * (m * k))
+            B = PK.from_ints([rng.getrandbits(3000) for _ in range(k * n)])
+        elif kind == 1:  # 1 x 1 x 1
+            m = k = n = 1
+            A = PK.from_ints([-rng.getrandbits(5000)])
+            B = PK.from_ints([rng.getrandbits(5000)])
+        else:
+            A = PK.from_ints([rng.choice([0, 1, -1]) * rng.getrandbits(rng.choice([1, 64, 4000]))
+                              for _ in range(m * k)])
+            B = PK.from_ints([rng.choice([0, 1, -1]) * rng.getrandbits(rng.choice([1, 64, 4000]))
+                              for _ in range(k * n)])
+        prods.append((m, k, n, A, B))
+    outs = api.matmul_batch(prods)
+    assert api.batch_stats()["chunks"] >= 2
+    for (m, k, n, A, B), C in zip(prods, outs):
+        a, b = A.to_ints(), B.to_ints()
+        want = [sum(a[i * k + l] * b[l * n + j] for l in range(k))
+                for i in range(m) for j in range(n)]
+        assert C.to_ints() == want
