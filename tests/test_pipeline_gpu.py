@@ -243,6 +243,7 @@ def test_pipeline_edge_cases(small_chunks):
             B = PK.from_ints([rng.choice([0, 1, -1]) * rng.getrandbits(rng.choice([1, 64, 4000]))
                               for _ in range(k * n)])
         prods.append((m, k, n, A, B))
+    api.set_chunk_limbs(1000)  # the whole batch is a few thousand limbs
     outs = api.matmul_batch(prods)
     assert api.batch_stats()["chunks"] >= 2
     for (m, k, n, A, B), C in zip(prods, outs):
