@@ -205,6 +205,27 @@ MPZMM_API int mpzmm_chain(int count, const mpzmm_matrix *mats, uint64_t *c_limbs
                           const int64_t *c_offs, const int64_t *c_caps, int32_t *c_sizes,
                           void *stream);
 
+/* ---- modular reduction by a fixed modulus ----
+   Counterpart of the reference's mpzfft_mod_init / mpzfft_mod_mod /
+   mpzfft_mod_clear (src/include/mpzfft.h, src/lib/mpzfft.c:59-100), which
+   reduce by one modulus d many times through a precomputed Fermat-transform
+   reciprocal.  Here: a Barrett reduction whose two big products run on this
+   library's engine, batched over all the x of a call.  mpzmm_mod_create
+   takes d > 0 (d_size limbs) and the largest |x| to expect in limbs
+   (max_x_limbs; larger x are refused with MPZMM_ERR_TOO_LARGE).
+   mpzmm_mod_batch writes r_i = x_i mod d in [0, d) for `count` packed x
+   (signed, as above) into packed outputs with capacity r_caps (d's limb count
+   always suffices, mpzmm_mod_limbs).  Synchronous. */
+typedef struct mpzmm_mod mpzmm_mod;
+MPZMM_API int mpzmm_mod_create(mpzmm_mod **mod, const uint64_t *d_limbs, int32_t d_size,
+                               int64_t max_x_limbs);
+MPZMM_API int64_t mpzmm_mod_limbs(const mpzmm_mod *mod);
+MPZMM_API int mpzmm_mod_batch(mpzmm_mod *mod, int count, const uint64_t *x_limbs,
+                              const int64_t *x_offs, const int32_t *x_sizes, uint64_t *r_limbs,
+                              const int64_t *r_offs, const int64_t *r_caps, int32_t *r_sizes,
+                              void *stream);
+MPZMM_API void mpzmm_mod_destroy(mpzmm_mod *mod);
+
 /* ---- device-resident plans (build once, run many times) ---- */
 typedef struct mpzmm_plan mpzmm_plan;
 

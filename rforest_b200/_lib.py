@@ -115,6 +115,10 @@ def lib():
         "mpzmm_batch_stats": (C.c_int, [i64p, i64p, i64p]),
         "mpzmm_chain_output_limbs": (C.c_int64, [C.c_int, C.POINTER(Matrix)]),
         "mpzmm_chain": (C.c_int, [C.c_int, C.POINTER(Matrix), u64p, i64p, i64p, i32p, vp]),
+        "mpzmm_mod_create": (C.c_int, [C.POINTER(vp), u64p, C.c_int32, C.c_int64]),
+        "mpzmm_mod_limbs": (C.c_int64, [vp]),
+        "mpzmm_mod_batch": (C.c_int, [vp, C.c_int, u64p, i64p, i32p, u64p, i64p, i64p, i32p, vp]),
+        "mpzmm_mod_destroy": (None, [vp]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

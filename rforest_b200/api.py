@@ -14,7 +14,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _lib
-from .packed import Packed
+from .packed import Packed, from_ints
 
 ProductIn = Tuple[int, int, int, Packed, Packed]
 
@@ -264,6 +264,51 @@ def chain(mats: Sequence[Tuple[int, int, Packed]], stream=None) -> Packed:
                                       _ptr(caps, _lib.i64p), _ptr(csz, _lib.i32p),
                                       _stream_arg(stream)))
     return Packed(cl, co, csz)
+
+
+class Mod:
+    """Reduction by a fixed modulus d > 0 (a Python int): ``reduce(X)`` gives
+    x mod d in [0, d) for every entry of the packed vector X, for entries of
+    up to ``max_bits`` bits.  Mirrors mpzfft_mod_init / mpzfft_mod_mod."""
+
+    def __init__(self, d: int, max_bits: int):
+        if d <= 0:
+            raise ValueError("the modulus must be positive")
+        self._d = from_ints([d])
+        self._dl = np.ascontiguousarray(self._d.limbs, dtype=np.uint64)
+        self.handle = C.c_void_p()
+        _lib.check(_lib.lib().mpzmm_mod_create(C.byref(self.handle), _ptr(self._dl, _lib.u64p),
+                                               int(self._d.sizes[0]), (int(max_bits) + 63) // 64))
+        self.n = int(_lib.lib().mpzmm_mod_limbs(self.handle))
+
+    def reduce(self, X: Packed, stream=None) -> Packed:
+        count = len(X)
+        xl = np.ascontiguousarray(X.limbs, dtype=np.uint64)
+        if xl.size == 0:
+            xl = np.zeros(1, np.uint64)
+        xo = np.ascontiguousarray(X.offs, dtype=np.int64)
+        xs = np.ascontiguousarray(X.sizes, dtype=np.int32)
+        rl = np.zeros(max(count * self.n, 1), dtype=np.uint64)
+        ro = np.arange(count, dtype=np.int64) * self.n
+        rc = np.full(count, self.n, dtype=np.int64)
+        rs = np.zeros(count, dtype=np.int32)
+        _lib.check(_lib.lib().mpzmm_mod_batch(self.handle, count, _ptr(xl, _lib.u64p),
+                                              _ptr(xo, _lib.i64p), _ptr(xs, _lib.i32p),
+                                              _ptr(rl, _lib.u64p), _ptr(ro, _lib.i64p),
+                                              _ptr(rc, _lib.i64p), _ptr(rs, _lib.i32p),
+                                              _stream_arg(stream)))
+        return Packed(rl, ro, rs)
+
+    def close(self) -> None:
+        if self.handle:
+            _lib.lib().mpzmm_mod_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Plan:

@@ -1027,6 +1027,139 @@ cudaError_t launch_fix_sizes(FwdDesc* descs, int count, const int32_t* sizes, cu
 }
 
 // ---------------------------------------------------------------------------
+// Modular reduction r = x mod d (Barrett, HAC 14.42 with B = 2^64): the two
+// big products run on the multiplication engine; these kernels shift sizes
+// between them and finish each x with one warp.
+// ---------------------------------------------------------------------------
+// out[i] = max(0, |in[i]| - shift): sizes of operands viewed `shift` limbs up
+__global__ void k_shift_sizes(const int32_t* __restrict__ in, int32_t* __restrict__ out,
+                              int count, int shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int32_t s = in[i];
+  const int32_t a = s < 0 ? -s : s;
+  out[i] = a > shift ? a - shift : 0;
+}
+
+cudaError_t launch_shift_sizes(const int32_t* in, int32_t* out, int count, int shift,
+                               cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  k_shift_sizes<<<(count + 255) / 256, 256, 0, st>>>(in, out, count, shift);
+  return cudaGetLastError();
+}
+
+namespace {
+// One 32-limb step of a - b - bin over the warp (limb `lane`): returns the
+// difference limb; *bstep carries the borrow into the next step.
+__device__ __forceinline__ uint64_t warp_sub_step(uint64_t a, uint64_t b, uint32_t* bstep) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  // borrow transfer per limb: out = g | (p & in)
+  uint32_t g = a < b ? 1u : 0u, pp = a == b ? 1u : 0u;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t gu = __shfl_up_sync(FULL, g, off), pu = __shfl_up_sync(FULL, pp, off);
+    if (lane >= off) {
+      g = g | (pp & gu);
+      pp = pp & pu;
+    }
+  }
+  const uint32_t out = g | (pp & *bstep);  // borrow out of this limb
+  uint32_t in = __shfl_up_sync(FULL, out, 1);
+  if (lane == 0) in = *bstep;
+  *bstep = __shfl_sync(FULL, out, 31);
+  return a - b - (uint64_t)in;
+}
+
+// r >= d over limbs [0, nl) (d is zero from limb nd on), warp-wide
+__device__ __forceinline__ bool warp_geq(const uint64_t* r, const uint64_t* d, int nl, int nd) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  for (int j0 = ((nl - 1) >> 5) << 5; j0 >= 0; j0 -= 32) {
+    const int j = j0 + lane;
+    const uint64_t a = j < nl ? r[j] : 0, b = j < nd ? d[j] : 0;
+    const unsigned diff = __ballot_sync(FULL, a != b);
+    if (diff) {
+      const int top = 31 - __clz(diff);
+      return __shfl_sync(FULL, a > b ? 1 : 0, top) != 0;
+    }
+  }
+  return true;  // equal
+}
+}  // namespace
+
+// r_i = x_i mod d in [0, d): r = (|x| - s) mod B^(n+1) with s = q d and q at
+// most 2 below floor(|x| / d), then up to two subtractions of d, then d - r
+// for a negative x with r != 0.  One warp per x; rbuf holds n + 1 limbs per x.
+__global__ void __launch_bounds__(128)
+k_mod_finish(int count, int n, const uint64_t* __restrict__ xl, const int64_t* __restrict__ xo,
+             const int32_t* __restrict__ xs, const uint64_t* __restrict__ sl, int64_t s_stride,
+             const int32_t* __restrict__ ss, const uint64_t* __restrict__ d,
+             uint64_t* __restrict__ rbuf, int32_t* __restrict__ rs) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= count) return;  // whole warp
+  const int nl = n + 1;
+  const int32_t xsz = xs[i];
+  const bool neg = xsz < 0;
+  const int xa = neg ? -xsz : xsz;
+  const int sa = ss[i] < 0 ? -ss[i] : ss[i];
+  const uint64_t* x = xl + xo[i];
+  const uint64_t* s = sl + (int64_t)i * s_stride;
+  uint64_t* r = rbuf + (int64_t)i * nl;
+  uint32_t b = 0;
+  for (int j0 = 0; j0 < nl; j0 += 32) {  // r = |x| - s mod B^(n+1)
+    const int j = j0 + lane;
+    const uint64_t a = (j < xa && j < nl) ? x[j] : 0, c = (j < sa && j < nl) ? s[j] : 0;
+    const uint64_t v = warp_sub_step(a, c, &b);
+    if (j < nl) r[j] = v;
+  }
+  __syncwarp();
+  for (int rep = 0; rep < 2; ++rep) {  // r < 3d: at most two subtractions
+    if (!warp_geq(r, d, nl, n)) break;
+    b = 0;
+    for (int j0 = 0; j0 < nl; j0 += 32) {
+      const int j = j0 + lane;
+      const uint64_t a = j < nl ? r[j] : 0, c = j < n ? d[j] : 0;
+      const uint64_t v = warp_sub_step(a, c, &b);
+      if (j < nl) r[j] = v;
+    }
+    __syncwarp();
+  }
+  // size, and d - r for a negative x with r != 0
+  int top = -1;
+  for (int j0 = 0; j0 < nl; j0 += 32) {
+    const int j = j0 + lane;
+    const unsigned nz = __ballot_sync(FULL, j < nl && r[j] != 0);
+    if (nz) top = j0 + 31 - __clz(nz);
+  }
+  if (neg && top >= 0) {
+    b = 0;
+    top = -1;
+    for (int j0 = 0; j0 < nl; j0 += 32) {
+      const int j = j0 + lane;
+      const uint64_t a = j < n ? d[j] : 0, c = j < nl ? r[j] : 0;
+      const uint64_t v = warp_sub_step(a, c, &b);
+      if (j < nl) r[j] = v;
+      const unsigned nz = __ballot_sync(FULL, j < nl && v != 0);
+      if (nz) top = j0 + 31 - __clz(nz);
+    }
+  }
+  if (lane == 0) rs[i] = top + 1;
+}
+
+cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_t* xo,
+                              const int32_t* xs, const uint64_t* sl, int64_t s_stride,
+                              const int32_t* ss, const uint64_t* d, uint64_t* rbuf, int32_t* rs,
+                              cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  k_mod_finish<<<(count + 3) / 4, 128, 0, st>>>(count, n, xl, xo, xs, sl, s_stride, ss, d, rbuf,
+                                                rs);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 cudaError_t upload_constants(const PrimeConst* primes, const CrtConst* crt) {

@@ -38,6 +38,14 @@ int contract_block_freqs();
 // writes the device-held signed sizes (and coefficient counts) of `count`
 // forward descriptors
 cudaError_t launch_fix_sizes(FwdDesc* descs, int count, const int32_t* sizes, cudaStream_t st);
+// modular reduction helpers: sizes of operands viewed `shift` limbs up, and
+// the final step of x mod d (see mod.cpp)
+cudaError_t launch_shift_sizes(const int32_t* in, int32_t* out, int count, int shift,
+                               cudaStream_t st);
+cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_t* xo,
+                              const int32_t* xs, const uint64_t* sl, int64_t s_stride,
+                              const int32_t* ss, const uint64_t* d, uint64_t* rbuf, int32_t* rs,
+                              cudaStream_t st);
 
 // Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
 // k <= 64, n <= 64; each work item covers `fb` consecutive frequencies.
