@@ -407,6 +407,7 @@ def main():
     if world == 1 and not args.no_compare and args.workload == "config3":
         comparisons = compare_forms(api, torch, stream, triples, args)
         api.set_contract_mode(modes[args.contract])
+        comparisons["mod_reduction"] = mod_benchmark(api)
 
     if rank == 0:
         # roofline of the dominant stage (3-pass model, reference parameters)
@@ -543,6 +544,44 @@ def compare_forms(api, torch, stream, triples, args):
     out["config2_chain"] = {"device_resident_ms": t_dev * 1e3, "host_round_trips_ms": t_host * 1e3,
                             "same_result": PK.digest(C) == PK.digest(M),
                             "timing": "wall clock, 15 products, inputs and result in host memory"}
+    return out
+
+
+def mod_benchmark(api):
+    """x mod d beside the product (a remainder-tree step): 2048 signed x of
+    2^17 bits by one d of 2^16 bits, through mpzmm_mod_batch (host arrays in,
+    host arrays out, wall clock), against the reference's own CPU
+    mpzfft_mod_mod (one core) on the first 32 x."""
+    from rforest_b200 import packed as PK, workloads as W
+    dbits, xbits, count = 1 << 16, 1 << 17, 2048
+    d = W.random_matrix(7001, 0, 0, 1, 1, dbits, False).entry(0) | (1 << (dbits - 1))
+    X = W.random_matrix(7001, 1, 0, count, 1, xbits, True)
+    xs = X.to_ints()
+    m = api.Mod(d, xbits)
+    try:
+        R = m.reduce(X)  # warm the workspaces
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            R = m.reduce(X)
+        gpu = count * reps / (time.perf_counter() - t0)
+    finally:
+        m.close()
+    out = {"workload": f"{count} signed x of 2^17 bits mod one d of 2^16 bits",
+           "value": gpu, "unit": "reductions/s", "timing": "wall clock, host arrays in and out",
+           "checked": R.slice(0, 16).to_ints() == [x % d for x in xs[:16]]}
+    try:
+        from oracle import oracle as O
+        if O.reference_available():
+            sample = PK.from_ints(xs[:32])
+            t0 = time.perf_counter()
+            ref = O.mod_reference(d, sample, xbits)
+            out["cpu_reference"] = {"value": 32 / (time.perf_counter() - t0),
+                                    "unit": "reductions/s", "cores": 1,
+                                    "kind": "reference mpzfft_mod_mod", "sample": "first 32 x"}
+            out["matches_reference"] = PK.digest(ref) == PK.digest(R.slice(0, 32))
+    except Exception as e:  # the comparison is informative only
+        out["cpu_reference"] = {"unavailable": str(e)[:200]}
     return out
 
 

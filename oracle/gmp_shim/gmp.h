@@ -110,6 +110,9 @@ mp_limb_t __gmpn_neg(mp_ptr, mp_srcptr, mp_size_t);
 int __gmpn_cmp(mp_srcptr, mp_srcptr, mp_size_t);
 void __gmpn_zero(mp_ptr, mp_size_t);
 void __gmpn_copyi(mp_ptr, mp_srcptr, mp_size_t);
+mp_limb_t __gmpn_add(mp_ptr, mp_srcptr, mp_size_t, mp_srcptr, mp_size_t);
+mp_limb_t __gmpn_sub(mp_ptr, mp_srcptr, mp_size_t, mp_srcptr, mp_size_t);
+void __gmpn_tdiv_qr(mp_ptr, mp_ptr, mp_size_t, mp_srcptr, mp_size_t, mp_srcptr, mp_size_t);
 
 #define mpn_add_n __gmpn_add_n
 #define mpn_sub_n __gmpn_sub_n
@@ -124,6 +127,9 @@ void __gmpn_copyi(mp_ptr, mp_srcptr, mp_size_t);
 #define mpn_cmp __gmpn_cmp
 #define mpn_zero __gmpn_zero
 #define mpn_copyi __gmpn_copyi
+#define mpn_add __gmpn_add
+#define mpn_sub __gmpn_sub
+#define mpn_tdiv_qr __gmpn_tdiv_qr
 
 /* ---- misc ---- */
 void __gmp_set_memory_functions(void *(*)(size_t),

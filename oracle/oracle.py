@@ -69,6 +69,9 @@ def _load_ref():
         lib.ref_matmul.argtypes = _MATMUL_ARGS
         lib.ref_matmul.restype = C.c_int
         lib.ref_setup.argtypes = []
+        lib.ref_mod.argtypes = [_u64p, C.c_int32, C.c_int64, C.c_int, _u64p, _i64p, _i32p,
+                                _u64p, _i64p, _i64p, _i32p]
+        lib.ref_mod.restype = C.c_int
         _ref = lib
     return _ref
 
@@ -115,6 +118,31 @@ def matmul_schoolbook(m, k, n, A, B):
 def matmul_reference(m, k, n, A, B):
     """C = A*B with the reference's own CPU mpz_rmatrix_mult_fft."""
     return _call(_load_ref().ref_matmul, m, k, n, A, B)
+
+
+def mod_reference(d: int, X, bits: int):
+    """x mod d in [0, d) for every entry of packed X with the reference's own
+    CPU mpzfft_mod_init / mpzfft_mod_mod (|x| and d of at most `bits` bits)."""
+    from rforest_b200.packed import Packed, from_ints
+    D = from_ints([d])
+    n = int(D.sizes[0])
+    count = len(X)
+    dl = np.ascontiguousarray(D.limbs, dtype=np.uint64)
+    xl = np.ascontiguousarray(X.limbs, dtype=np.uint64)
+    if xl.size == 0:
+        xl = np.zeros(1, np.uint64)
+    xo = np.ascontiguousarray(X.offs, dtype=np.int64)
+    xs = np.ascontiguousarray(X.sizes, dtype=np.int32)
+    out = np.zeros(max(count * n, 1), dtype=np.uint64)
+    offs = np.arange(count, dtype=np.int64) * n
+    caps = np.full(count, n, dtype=np.int64)
+    sizes = np.zeros(count, dtype=np.int32)
+    st = _load_ref().ref_mod(_ptr(dl, _u64p), n, int(bits), count, _ptr(xl, _u64p),
+                             _ptr(xo, _i64p), _ptr(xs, _i32p), _ptr(out, _u64p),
+                             _ptr(offs, _i64p), _ptr(caps, _i64p), _ptr(sizes, _i32p))
+    if st != 0:
+        raise RuntimeError("oracle output capacity too small")
+    return Packed(out, offs, sizes)
 
 
 def reference_params(maxlimbs: int, terms: int):

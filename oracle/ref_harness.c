@@ -14,6 +14,7 @@
 #include <string.h>
 #include "gmp.h"
 #include "hwmpz.h"
+#include "mpzfft.h"
 
 static int ref_ready;
 
@@ -78,5 +79,48 @@ int ref_matmul(int m, int k, int n, const uint64_t *a_limbs,
   free(A);
   free(B);
   free(C);
+  return status;
+}
+
+/* x mod d in [0, d) for `count` packed x through the reference's own
+ * mpzfft_mod_init / mpzfft_mod_mod (src/lib/mpzfft.c:59-100; Fermat-transform
+ * reciprocal, src/lib/mpnfft_mod.c:283-476) with 4 FFT primes, as hwmpz.c
+ * uses for the product.  `bits` bounds |x| (and d's bit length).  Returns 0,
+ * or -1 if an output capacity is too small. */
+static zz_moduli_t mod_moduli;
+static int mod_moduli_ready;
+
+int ref_mod(const uint64_t *d_limbs, int32_t d_size, int64_t bits, int count,
+            const uint64_t *x_limbs, const int64_t *x_offs, const int32_t *x_sizes,
+            uint64_t *r_limbs, const int64_t *r_offs, const int64_t *r_caps,
+            int32_t *r_sizes) {
+  if (!mod_moduli_ready) {
+    zz_moduli_init(&mod_moduli, 4);
+    mod_moduli_ready = 1;
+  }
+  mpz_t d, x, r;
+  mpz_init(d);
+  mpz_init(x);
+  mpz_init(r);
+  load(d, d_limbs, 0, d_size);
+  mpzfft_mod_t M;
+  mpzfft_mod_init(&M, (size_t)bits, d, 4, &mod_moduli, 1);
+  int status = 0;
+  for (int i = 0; i < count; i++) {
+    load(x, x_limbs, x_offs[i], x_sizes[i]);
+    mpzfft_mod_mod(&M, r, x, 1);
+    size_t sz = mpz_size(r);
+    if ((int64_t)sz > r_caps[i]) {
+      status = -1;
+      r_sizes[i] = 0;
+      continue;
+    }
+    if (sz) memcpy(r_limbs + r_offs[i], r->_mp_d, sz * 8);
+    r_sizes[i] = r->_mp_size;
+  }
+  mpzfft_mod_clear(&M);
+  mpz_clear(d);
+  mpz_clear(x);
+  mpz_clear(r);
   return status;
 }

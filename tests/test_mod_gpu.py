@@ -61,3 +61,21 @@ def test_too_large_and_bad_modulus(gpu):
         m.close()
     with pytest.raises(ValueError):
         api.Mod(0, 64)
+
+
+def test_matches_reference_mod(gpu, oracle_mod):
+    """The GPU reduction against the reference's own CPU mpzfft_mod_mod."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference CPU build not present")
+    rng = random.Random(21)
+    for dbits in (64, 1000, 16384):
+        d = rng.getrandbits(dbits) | (1 << (dbits - 1))
+        bits = 2 * dbits
+        X = PK.from_ints([rng.choice([1, -1]) * rng.getrandbits(rng.randrange(1, bits + 1))
+                          for _ in range(50)])
+        m = api.Mod(d, bits)
+        try:
+            got = m.reduce(X)
+        finally:
+            m.close()
+        assert PK.digest(got) == PK.digest(oracle_mod.mod_reference(d, X, bits))

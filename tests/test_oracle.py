@@ -104,3 +104,18 @@ def test_reference_params_match_survey(oracle_mod):
     # (r, lgN, points) the reference picks for config 1 / config 2
     assert oracle_mod.reference_params(64, 4) == (119, 7, 71)
     assert oracle_mod.reference_params(1024, 8) == (117, 11, 1122)
+
+
+def test_reference_mod_pinned(oracle_mod):
+    """The reference's own CPU x mod d (mpzfft_mod_mod, Fermat-transform
+    reciprocal) against Python integers: the oracle of the GPU reduction."""
+    if not oracle_mod.reference_available():
+        pytest.skip("reference CPU build not present")
+    rng = random.Random(13)
+    for dbits in (1, 63, 64, 65, 640, 4096, 30000):
+        d = rng.getrandbits(dbits) | (1 << (dbits - 1))
+        bits = 2 * dbits + 200
+        xs = [0, 1, -1, d, -d, d - 1, 3 * d + 5]
+        xs += [rng.choice([1, -1]) * rng.getrandbits(rng.randrange(1, bits)) for _ in range(40)]
+        R = oracle_mod.mod_reference(d, PK.from_ints(xs), bits)
+        assert R.to_ints() == [x % d for x in xs], dbits
