@@ -225,6 +225,10 @@ MPZMM_API int mpzmm_mod_batch(mpzmm_mod *mod, int count, const uint64_t *x_limbs
                               const int64_t *r_offs, const int64_t *r_caps, int32_t *r_sizes,
                               void *stream);
 MPZMM_API void mpzmm_mod_destroy(mpzmm_mod *mod);
+/* The same over mpz_t arrays: rop[i] = op[i] mod d for i < count, each rop
+   grown with mpz_realloc (the reference's mpzfft_mod_mod, batched; rop may
+   alias op). */
+MPZMM_API int mpzmm_mod_mpz(mpzmm_mod *mod, mpz_t *rop, mpz_t *op, int count, void *stream);
 
 /* ---- device-resident plans (build once, run many times) ---- */
 typedef struct mpzmm_plan mpzmm_plan;

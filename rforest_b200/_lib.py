@@ -119,6 +119,7 @@ def lib():
         "mpzmm_mod_limbs": (C.c_int64, [vp]),
         "mpzmm_mod_batch": (C.c_int, [vp, C.c_int, u64p, i64p, i32p, u64p, i64p, i64p, i32p, vp]),
         "mpzmm_mod_destroy": (None, [vp]),
+        "mpzmm_mod_mpz": (C.c_int, [vp, vp, vp, C.c_int, vp]),
         "mpzmm_choose_params": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     }

@@ -271,4 +271,35 @@ int mpzmm_mod_batch(mpzmm_mod* m, int count, const uint64_t* x_limbs, const int6
   return status;
 }
 
+// mpz_t front end: rop[i] = op[i] mod d in [0, d), grown with GMP's own
+// allocator like the reference's mpzfft_mod_mod (src/lib/mpzfft.c:73-100)
+int mpzmm_mod_mpz(mpzmm_mod* m, mpz_t* rop, mpz_t* op, int count, void* stream) {
+  if (!m) return set_error(kErrArg, "null modulus");
+  if (count < 0 || (count > 0 && (!rop || !op))) return set_error(kErrArg, "bad mpz arrays");
+  if (count == 0) return kOk;
+  std::vector<int64_t> xo((size_t)count), ro((size_t)count), rc((size_t)count, m->n);
+  std::vector<int32_t> xs((size_t)count), rs((size_t)count);
+  size_t tot = 0;
+  for (int i = 0; i < count; ++i) {
+    xo[i] = (int64_t)tot;
+    xs[i] = op[i]->_mp_size;
+    tot += (size_t)std::llabs((long long)op[i]->_mp_size);
+  }
+  std::vector<uint64_t> xl(tot ? tot : 1), rl((size_t)count * m->n);
+  for (int i = 0; i < count; ++i)
+    if (xs[i])
+      std::memcpy(xl.data() + xo[i], op[i]->_mp_d, (size_t)std::llabs((long long)xs[i]) * 8);
+  for (int i = 0; i < count; ++i) ro[i] = (int64_t)i * m->n;
+  int st = mpzmm_mod_batch(m, count, xl.data(), xo.data(), xs.data(), rl.data(), ro.data(),
+                           rc.data(), rs.data(), stream);
+  if (st) return st;
+  for (int i = 0; i < count; ++i) {
+    __mpz_struct* z = rop[i];
+    if (z->_mp_alloc < rs[i]) __gmpz_realloc(z, (mp_size_t)rs[i]);
+    if (rs[i]) std::memcpy(z->_mp_d, rl.data() + ro[i], (size_t)rs[i] * 8);
+    z->_mp_size = rs[i];
+  }
+  return kOk;
+}
+
 }  // extern "C"

@@ -79,3 +79,21 @@ def test_matches_reference_mod(gpu, oracle_mod):
         finally:
             m.close()
         assert PK.digest(got) == PK.digest(oracle_mod.mod_reference(d, X, bits))
+
+
+def test_mpz_front_end(gpu):
+    """mpz_t arrays in and out (rop grown by GMP), rop aliasing op too."""
+    from rforest_b200 import gmp
+    rng = random.Random(31)
+    d = rng.getrandbits(3000) | (1 << 2999)
+    xs = [0, 7, -7, d, -(d + 1)] + [rng.choice([1, -1]) * rng.getrandbits(6000) for _ in range(20)]
+    m = api.Mod(d, 6000)
+    try:
+        X = gmp.MpzArray(xs)
+        R = gmp.MpzArray(n=len(xs))
+        _lib.check(_lib.lib().mpzmm_mod_mpz(m.handle, R.ptr(), X.ptr(), len(xs), None))
+        assert R.to_ints() == [x % d for x in xs]
+        _lib.check(_lib.lib().mpzmm_mod_mpz(m.handle, X.ptr(), X.ptr(), len(xs), None))
+        assert X.to_ints() == [x % d for x in xs]
+    finally:
+        m.close()
