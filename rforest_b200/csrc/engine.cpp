@@ -1168,7 +1168,7 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
 
   // chunks of consecutive whole products; the first two are a quarter and
   // a half of the others, so the first results start back sooner (the
-  // device->host copies are the pipeline's longest chain)
+  // device->host copies are the pipeline's longest chain),
   std::vector<size_t> bounds{0};
   uint64_t acc = 0;
   for (size_t t = 0; t < specs.size(); ++t) {
@@ -1181,6 +1181,19 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     }
   }
   bounds.push_back(specs.size());
+  // and the last one is split about 2:1, so the final results come back
+  // sooner after the last inputs went in
+  if (bounds.size() >= 3) {
+    const size_t a = bounds[bounds.size() - 2], b = bounds.back();
+    uint64_t tail = 0;
+    for (size_t t = a; t < b; ++t) tail += limbs[t];
+    if (tail > chunk / 2 && b - a >= 2) {
+      uint64_t acc2 = 0;
+      size_t cut = a;
+      while (cut + 1 < b && 3 * (acc2 + limbs[cut]) <= 2 * tail) acc2 += limbs[cut++];
+      if (cut > a) bounds.insert(bounds.end() - 1, cut);
+    }
+  }
   const size_t nchunks = bounds.size() - 1;
   ctx.batch_chunks = (int64_t)nchunks;
   int s = ensure_pipeline(ctx);
