@@ -385,6 +385,12 @@ def main():
     e2e_steps = max(1, args.e2e_steps)
     batch = api.Batch(triples, pinned=True)
     e2e_ms, e2e_stats = time_batch(batch, e2e_steps)
+    # the last timed step's chunks: planned, queued, copied in, computed and
+    # copied out (ms from the call's start), and MB each way
+    e2e_timeline = [[round(r[k], 2) for k in ("plan_end", "queue_end", "h2d_begin", "h2d_end",
+                                             "kernels_end", "d2h_end")]
+                    + [round(r["h2d_bytes"] / 1e6, 1), round(r["d2h_bytes"] / 1e6, 1)]
+                    for r in api.batch_timeline()]
     batch.close()
     del batch
     e2e_value = replicas.whole_job_rate(units_per_rank, world, e2e_steps, e2e_ms)
@@ -458,7 +464,10 @@ def main():
                                               e2e_stats["d2h_direct_bytes"]],
                     "host_ms_per_step": {k: round(v, 2)
                                          for k, v in e2e_stats.items() if k.endswith("_ms")},
-                    "pageable": e2e_pageable},
+                    "pageable": e2e_pageable,
+                    "timeline_fields": ["plan_end", "queue_end", "h2d_begin", "h2d_end",
+                                        "kernels_end", "d2h_end", "h2d_MB", "d2h_MB"],
+                    "timeline": e2e_timeline},
             "gpu_launches": int(sum(stage_launches) * args.steps),
             "value_cuda_graph": value_graph,
             "stages_ms_per_step": {n: round(t / max(1, timed), 4)

@@ -130,6 +130,17 @@ MPZMM_API int mpzmm_host_unregister(void *p);
    caller's pinned memory and the device. */
 MPZMM_API int mpzmm_batch_stats(int64_t *ns4, int64_t *chunks, int64_t *bytes4);
 
+/* Per-chunk timeline of the last one-shot batch: *nchunks gets its chunk
+   count and rows (may be NULL) up to max_chunks rows of
+   MPZMM_TIMELINE_FIELDS doubles, in ms from the batch's start: [0] planning
+   began, [1] planning ended, [2] queueing began, [3] queueing ended (host
+   clock); [4] the input copies could start (the copy stream reached them),
+   [5] input copies done, [6] kernels done, [7] result copies done (device
+   events, -1 where the batch failed before them); [8] bytes host->device,
+   [9] bytes device->host. */
+#define MPZMM_TIMELINE_FIELDS 10
+MPZMM_API int mpzmm_batch_timeline(double *rows, int max_chunks, int *nchunks);
+
 /* Autotuner: times the contraction of a representative product per size
    class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
    entries) on CUDA cores and on tensor cores and makes automatic mode use

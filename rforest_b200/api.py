@@ -76,6 +76,22 @@ def batch_stats():
             "h2d_direct_bytes": nb[2], "d2h_direct_bytes": nb[3]}
 
 
+TIMELINE_FIELDS = ("plan_begin", "plan_end", "queue_begin", "queue_end", "h2d_begin",
+                   "h2d_end", "kernels_end", "d2h_end", "h2d_bytes", "d2h_bytes")
+
+
+def batch_timeline():
+    """Last one-shot batch, one dict per chunk: host planning and queueing
+    times and device copy / kernel event times in ms from the batch's start,
+    and the bytes copied each way (mpzmm_batch_timeline)."""
+    n = C.c_int()
+    _lib.check(_lib.lib().mpzmm_batch_timeline(None, 0, C.byref(n)))
+    rows = (C.c_double * (len(TIMELINE_FIELDS) * max(1, n.value)))()
+    _lib.check(_lib.lib().mpzmm_batch_timeline(rows, n.value, C.byref(n)))
+    F = len(TIMELINE_FIELDS)
+    return [dict(zip(TIMELINE_FIELDS, rows[c * F:(c + 1) * F])) for c in range(n.value)]
+
+
 class HostArena:
     """Pinned host memory from the library (mpzmm_host_alloc).  Transfers
     whose host side lies inside it go straight to and from the device."""

@@ -1,4 +1,5 @@
 // extern "C" entry points of libmpzmm_b200.so (declared in include/mpzmm_b200.h).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
@@ -193,6 +194,20 @@ int mpzmm_batch_stats(int64_t* ns4, int64_t* chunks, int64_t* bytes4) {
     if (bytes4) bytes4[i] = context().batch_bytes[i];
   }
   if (chunks) *chunks = context().batch_chunks;
+  return kOk;
+}
+
+static_assert(MPZMM_TIMELINE_FIELDS == mpzmm::kTimelineFields, "timeline row size");
+
+int mpzmm_batch_timeline(double* rows, int max_chunks, int* nchunks) {
+  std::lock_guard<std::mutex> lk(workspace_mutex());
+  const std::vector<double>& tl = context().timeline;
+  const int n = (int)(tl.size() / kTimelineFields);
+  if (nchunks) *nchunks = n;
+  if (rows && max_chunks > 0) {
+    const int k = n < max_chunks ? n : max_chunks;
+    std::copy(tl.begin(), tl.begin() + (size_t)k * kTimelineFields, rows);
+  }
   return kOk;
 }
 

@@ -1125,6 +1125,31 @@ int ensure_pipeline(Context& ctx) {
     }
   return kOk;
 }
+
+// Timing events of a batch of n chunks (the start event and four a chunk)
+// and its timeline rows, zeroed.
+int ensure_timeline(Context& ctx, size_t nchunks) {
+  while (ctx.tl_ev.size() < 1 + 4 * nchunks) {
+    cudaEvent_t e = nullptr;
+    CU(cudaEventCreate(&e), "cudaEventCreate");
+    ctx.tl_ev.push_back(e);
+  }
+  ctx.timeline.assign(nchunks * kTimelineFields, 0.0);
+  return kOk;
+}
+
+// The device columns of the timeline, once every event of the batch is done.
+void read_timeline(Context& ctx, size_t nchunks) {
+  for (size_t c = 0; c < nchunks; ++c)
+    for (int k = 0; k < 4; ++k) {
+      float ms = -1.f;
+      if (cudaEventElapsedTime(&ms, ctx.tl_ev[0], ctx.tl_ev[1 + 4 * c + k]) != cudaSuccess) {
+        cudaGetLastError();
+        ms = -1.f;
+      }
+      ctx.timeline[c * kTimelineFields + 4 + k] = ms;
+    }
+}
 }  // namespace
 
 int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
@@ -1147,15 +1172,24 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
 
   if (specs.size() < 2 || total <= chunk) {
     ctx.batch_chunks = 1;
+    int s = ensure_timeline(ctx, 1);
+    if (s) return s;
+    double* tl = ctx.timeline.data();
+    const cudaEvent_t* ev = ctx.tl_ev.data();
     const int64_t t0 = now_ns();
+    s = cuda_status(cudaEventRecord(ev[0], st), "cudaEventRecord");
     Plan plan;
-    int s = plan.build(std::move(specs), ctx.ws);
+    if (!s) s = plan.build(std::move(specs), ctx.ws);
     if (!s) count_bytes(plan);
     const int64_t t1 = now_ns();
+    if (!s) s = cuda_status(cudaEventRecord(ev[1], st), "cudaEventRecord");
     if (!s) s = plan.upload(st);
+    if (!s) s = cuda_status(cudaEventRecord(ev[2], st), "cudaEventRecord");
     const int64_t t2 = now_ns();
     if (!s) s = plan.execute(st);
+    if (!s) s = cuda_status(cudaEventRecord(ev[3], st), "cudaEventRecord");
     if (!s) s = plan.download_enqueue(st);
+    if (!s) s = cuda_status(cudaEventRecord(ev[4], st), "cudaEventRecord");
     const int64_t t3 = now_ns();
     if (!s) s = plan.download_finish(st);
     const int64_t t4 = now_ns();
@@ -1163,6 +1197,15 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     ctx.batch_ns[1] = t2 - t1;
     ctx.batch_ns[2] = t3 - t2;
     ctx.batch_ns[3] = t4 - t3;
+    tl[0] = 0.0;
+    tl[1] = (t1 - t0) * 1e-6;
+    tl[2] = tl[1];
+    tl[3] = (t3 - t0) * 1e-6;
+    if (!s) {
+      tl[8] = (double)plan.upload_bytes();
+      tl[9] = (double)plan.download_bytes();
+      read_timeline(ctx, 1);
+    }
     return s;
   }
 
@@ -1197,12 +1240,17 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   const size_t nchunks = bounds.size() - 1;
   ctx.batch_chunks = (int64_t)nchunks;
   int s = ensure_pipeline(ctx);
+  if (!s) s = ensure_timeline(ctx, nchunks);
   if (s) return s;
+  double* tl = ctx.timeline.data();
+  const cudaEvent_t* ev = ctx.tl_ev.data();
   // the pipeline's streams start after the caller's earlier work
   CU(cudaEventRecord(ctx.pipe_ev, st), "cudaEventRecord");
   for (cudaStream_t ps : ctx.pipe_st) CU(cudaStreamWaitEvent(ps, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
   CU(cudaStreamWaitEvent(ctx.pipe_in, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
   CU(cudaStreamWaitEvent(ctx.pipe_out, ctx.pipe_ev, 0), "cudaStreamWaitEvent");
+  const int64_t tl0 = now_ns();
+  CU(cudaEventRecord(ev[0], ctx.pipe_in), "cudaEventRecord");
 
   // The caller's thread plans chunks and waits for finished ones; a
   // submitter thread queues each chunk's copies and kernels, because queueing
@@ -1233,19 +1281,26 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
       Plan* p = plans[w].get();
       cudaStream_t ps = ctx.pipe_st[w];
       const int64_t t0 = now_ns();
+      const cudaEvent_t* ce = ev + 1 + 4 * c;
       // copies in each direction in chunk order on their own stream; the
       // kernels of neighbouring chunks may overlap (one chunk's tail fills
       // in beside the next)
-      int r = p->upload(ctx.pipe_in);
+      int r = cuda_status(cudaEventRecord(ce[0], ctx.pipe_in), "cudaEventRecord");
+      if (!r) r = p->upload(ctx.pipe_in);
       if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_in[w], ctx.pipe_in), "cudaEventRecord");
+      if (!r) r = cuda_status(cudaEventRecord(ce[1], ctx.pipe_in), "cudaEventRecord");
       const int64_t t1 = now_ns();
       if (!r) r = cuda_status(cudaStreamWaitEvent(ps, ctx.pipe_ev_in[w], 0), "wait");
       if (!r) r = p->execute(ps);
       if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_exec[w], ps), "cudaEventRecord");
+      if (!r) r = cuda_status(cudaEventRecord(ce[2], ps), "cudaEventRecord");
       if (!r) r = cuda_status(cudaStreamWaitEvent(ctx.pipe_out, ctx.pipe_ev_exec[w], 0), "wait");
       if (!r) r = p->download_enqueue(ctx.pipe_out);
       if (!r) r = cuda_status(cudaEventRecord(ctx.pipe_ev_out[w], ctx.pipe_out), "cudaEventRecord");
+      if (!r) r = cuda_status(cudaEventRecord(ce[3], ctx.pipe_out), "cudaEventRecord");
       const int64_t t2 = now_ns();
+      tl[c * kTimelineFields + 2] = (t0 - tl0) * 1e-6;
+      tl[c * kTimelineFields + 3] = (t2 - tl0) * 1e-6;
       std::lock_guard<std::mutex> lk(mu);
       sub_ns[0] += t1 - t0;
       sub_ns[1] += t2 - t1;
@@ -1296,7 +1351,8 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     plans[w].reset(new Plan);
     const int64_t t0 = now_ns();
     const int r = plans[w]->build(std::move(part), ctx.pipe_ws[w]);
-    ctx.batch_ns[0] += now_ns() - t0;
+    const int64_t t1 = now_ns();
+    ctx.batch_ns[0] += t1 - t0;
     if (r) {
       if (!status) status = r;
       stop = true;
@@ -1304,6 +1360,11 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
       break;
     }
     count_bytes(*plans[w]);
+    double* row = tl + c * kTimelineFields;
+    row[0] = (t0 - tl0) * 1e-6;
+    row[1] = (t1 - tl0) * 1e-6;
+    row[8] = (double)plans[w]->upload_bytes();
+    row[9] = (double)plans[w]->download_bytes();
     slot_chunk[w] = c;
     std::lock_guard<std::mutex> lk(mu);
     queue.push_back(c);
@@ -1321,6 +1382,7 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   ctx.batch_ns[1] = sub_ns[0];
   ctx.batch_ns[2] = sub_ns[1];
   if (sub_status && (!status || status == kErrCapacity)) status = set_error(sub_status, sub_msg);
+  if (!status) read_timeline(ctx, nchunks);
   return status;
 }
 

@@ -144,7 +144,17 @@ struct Context {
   int64_t batch_ns[4] = {0, 0, 0, 0};
   int64_t batch_chunks = 0;
   int64_t batch_bytes[4] = {0, 0, 0, 0};
+  // per-chunk timeline of the last one-shot batch, kTimelineFields values a
+  // chunk (see mpzmm_batch_timeline); tl_ev: the batch's start event and
+  // four per chunk, with timing
+  std::vector<double> timeline;
+  std::vector<cudaEvent_t> tl_ev;
 };
+
+// Values per chunk in a batch timeline: plan begin / end, submit begin /
+// end (host, ms), copy-in begin / end, kernels end, copy-out end (device,
+// ms), bytes in, bytes out.
+constexpr int kTimelineFields = 10;
 
 // Chunks in flight in a pipelined one-shot batch.
 constexpr int kPipeDepth = 4;

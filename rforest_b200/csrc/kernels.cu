@@ -341,37 +341,56 @@ __device__ __forceinline__ uint32_t word_tf(uint32_t y, int g) {
 //     c mod p = REDC( sum_q d_q * (2^(30 q + 32) mod p) )
 // (D products of 30-bit by 30-bit numbers, exact in 64 bits for D <= 8), so
 // each prime costs D wide multiply-adds and one Montgomery reduction instead
-// of a Horner chain.  Larger transforms take a whole CTA and re-extract
-// digits per prime.  Then passes of 3 stages in registers (ntt_fast.cuh).
+// of a Horner chain.  Larger transforms take a whole CTA; their digits are
+// extracted once into shared memory when it has room (else per prime).  Then
+// passes of 3 stages in registers (ntt_fast.cuh).
 // ---------------------------------------------------------------------------
 constexpr int kFwdThreads = 256;
+// dynamic shared memory of a whole-CTA forward launch up to which its
+// digits are cached (three CTAs still fit an SM)
+constexpr int kFwdCacheBytes = 72 * 1024;
 
+// Digits of the coefficient starting at bit bit0 (r bits of the entry's nw
+// 32-bit words; bits past the entry read as 0).  Bit positions fit 32 bits:
+// a transform has at most 2^15 coefficients of at most 210 bits.
 template <int D>
-__device__ __forceinline__ void coeff_digits(const uint32_t* __restrict__ w32, uint64_t nw,
-                                             uint64_t bit0, uint32_t r, bool live,
+__device__ __forceinline__ void coeff_digits(const uint32_t* __restrict__ w32, uint32_t nw,
+                                             uint32_t bit0, uint32_t r, bool live,
                                              uint32_t (&dg)[D]) {
+  // every word the D digits touch lies inside the entry (the usual case)
+  const bool inside = live && ((bit0 + 30u * (D - 1)) >> 5) + 2u <= nw;
 #pragma unroll
   for (int q = 0; q < D; ++q) {
-    const uint64_t b = bit0 + 30u * q;
-    const uint64_t wi = b >> 5;
-    const uint32_t sh = (uint32_t)(b & 31);
-    const uint32_t lo = (live && wi < nw) ? __ldg(w32 + wi) : 0u;
-    const uint32_t hi = (live && wi + 1 < nw) ? __ldg(w32 + wi + 1) : 0u;
-    uint32_t v = __funnelshift_r(lo, hi, sh) & 0x3fffffffu;
+    const uint32_t b = bit0 + 30u * q;
+    const uint32_t wi = b >> 5;
+    uint32_t lo, hi;
+    if (inside) {
+      lo = __ldg(w32 + wi);
+      hi = __ldg(w32 + wi + 1);
+    } else {
+      lo = (live && wi < nw) ? __ldg(w32 + wi) : 0u;
+      hi = (live && wi + 1 < nw) ? __ldg(w32 + wi + 1) : 0u;
+    }
+    uint32_t v = __funnelshift_r(lo, hi, b & 31u) & 0x3fffffffu;
     const int rem = (int)r - 30 * q;  // bits of the coefficient left for this digit
     if (rem < 30) v = rem <= 0 ? 0u : (v & ((1u << rem) - 1u));
     dg[q] = v;
   }
 }
 
+// The residue of a coefficient from its digits, lazily reduced: the REDC
+// of S = sum_q d_q (2^(30q+32) mod p) < D 2^30 p is below (D/4 + 1) p < 3p
+// for D <= 7, and a negative entry's residue is taken as 3p - v, in (0, 3p]:
+// both below 4p, the forward transform's input range.
 template <int D>
 __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int j, bool neg) {
   const uint32_t p = c_primes[j].p;
   uint64_t S = 0;
 #pragma unroll
   for (int q = 0; q < D; ++q) S += (uint64_t)dg[q] * c_primes[j].dig[q];
-  const uint32_t v = redc64(S, p, c_primes[j].pinv, c_primes[j].mu);
-  return (neg && v) ? p - v : v;
+  const uint32_t m = (uint32_t)S * c_primes[j].pinv;
+  const uint32_t v = (uint32_t)((S + (uint64_t)m * p) >> 32);
+  return neg ? 3u * p - v : v;
 }
 
 // 2^L consecutive points reduced from [0, 4p) to [0, p), vector stores
@@ -409,26 +428,40 @@ __device__ __forceinline__ void fwd_last_pass(const uint32_t* s, uint32_t* out, 
 // The body of k_fwd2.  HZ: every polynomial of the CTA has at most N/2
 // coefficients (the usual case: both factors of a product fit in N
 // together), so the first pass's upper four points are zero: their digits
-// and residues are skipped and stage 0 only copies.
+// and residues are skipped and stage 0 only copies.  dig (whole-CTA HZ
+// transforms, NULL otherwise): shared memory for the entry's digits, digit q
+// of coefficient x at dig[q N/2 + x], extracted once for all P primes.
 template <int D, bool TEAM, bool HZ>
-__device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, bool valid, int lgN, int P,
-                                         int tt, int TS, const uint64_t* __restrict__ limbs,
+__device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t* dig,
+                                         bool valid, int lgN, int P, int tt, int TS,
+                                         const uint64_t* __restrict__ limbs,
                                          uint32_t* __restrict__ res,
                                          const uint2* __restrict__ twf) {
   const int N = 1 << lgN;
-  const uint64_t nw = 2ull * (uint64_t)(d.size < 0 ? -d.size : d.size);
+  const uint32_t nl = (uint32_t)(d.size < 0 ? -d.size : d.size);
+  const uint32_t nw = nl < 0x40000000u ? 2u * nl : 0x80000000u;
   const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
   const bool neg = d.size < 0;
   const int ng0 = N >> 3;  // groups (and the point stride) of the first pass
   constexpr int QN = HZ ? 4 : 8;  // points of a first-pass group that can be nonzero
+  const bool cached = !TEAM && HZ && dig != nullptr;
 
   uint32_t dg[QN][D];
   if (TEAM) {
 #pragma unroll
     for (int q = 0; q < QN; ++q) {
       const int x = q * ng0 + tt;
-      coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
+      coeff_digits<D>(w32, nw, (uint32_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
     }
+  } else if (cached) {
+    const int half = N >> 1;
+    for (int x = tt; x < half; x += TS) {
+      uint32_t t[D];
+      coeff_digits<D>(w32, nw, (uint32_t)x * d.r, d.r, (uint32_t)x < d.ncoef, t);
+#pragma unroll
+      for (int q = 0; q < D; ++q) dig[q * half + x] = t[q];
+    }
+    __syncthreads();
   }
   for (int j = 0; j < P; ++j) {
     const uint32_t p = c_primes[j].p;
@@ -439,8 +472,14 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, bool val
 #pragma unroll
       for (int q = 0; q < QN; ++q) {
         const int x = q * ng0 + g;
-        if (!TEAM)
-          coeff_digits<D>(w32, nw, (uint64_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
+        if (!TEAM) {
+          if (cached) {
+#pragma unroll
+            for (int u = 0; u < D; ++u) dg[q][u] = dig[u * (N >> 1) + x];
+          } else {
+            coeff_digits<D>(w32, nw, (uint32_t)x * d.r, d.r, (uint32_t)x < d.ncoef, dg[q]);
+          }
+        }
         a[q] = digits_residue<D>(dg[q], j, neg);
       }
       if (HZ) {
@@ -474,11 +513,14 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, bool val
   }
 }
 
+// dig_words: shared memory words after the transform reserved for the digit
+// cache of a whole-CTA launch (0: none); it holds D N/2 words for the CTA's
+// transform size.
 template <int D, bool TEAM>
 __global__ void __launch_bounds__(kFwdThreads, 3)
 k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
        const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
-       uint32_t* __restrict__ res, const uint2* __restrict__ twf) {
+       uint32_t* __restrict__ res, const uint2* __restrict__ twf, int dig_words) {
   extern __shared__ uint32_t sm[];
   const CtaItem item = items[blockIdx.x];
   const int lgN = item.lgN;
@@ -489,6 +531,7 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   const int tt = TEAM ? (int)threadIdx.x % TS : (int)threadIdx.x;
   const bool valid = team < (int)item.count;
   uint32_t* s = sm + team * (N + (N >> 5));
+  uint32_t* dig = (!TEAM && dig_words >= D * (N >> 1)) ? s + N + (N >> 5) : nullptr;
   FwdDesc d;
   d.limb_off = 0;
   d.res_off = 0;
@@ -498,9 +541,9 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   if (valid) d = descs[idx[item.first + team]];
   // one variant for the whole CTA (its barriers must be the same code)
   if (__syncthreads_and(d.ncoef <= (uint32_t)(N >> 1)))
-    fwd_body<D, TEAM, true>(d, s, valid, lgN, P, tt, TS, limbs, res, twf);
+    fwd_body<D, TEAM, true>(d, s, dig, valid, lgN, P, tt, TS, limbs, res, twf);
   else
-    fwd_body<D, TEAM, false>(d, s, valid, lgN, P, tt, TS, limbs, res, twf);
+    fwd_body<D, TEAM, false>(d, s, nullptr, valid, lgN, P, tt, TS, limbs, res, twf);
 }
 
 // Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
@@ -1179,12 +1222,21 @@ static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
                                  const uint64_t* limbs, uint32_t* res, const uint2* twf,
                                  cudaStream_t st) {
   const int Nmax = 1 << max_lgN;
-  const size_t smem = team ? sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5))
-                           : sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
   if (team) {
-    k_fwd2<D, true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
+    const size_t smem = sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5));
+    k_fwd2<D, true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf, 0);
   } else {
-    k_fwd2<D, false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf);
+    // whole-CTA transforms: the digit cache when the launch still fits
+    // three CTAs an SM with it (every CTA's transform is at most Nmax)
+    size_t smem = sizeof(uint32_t) * (size_t)(Nmax + (Nmax >> 5));
+    const size_t cache = sizeof(uint32_t) * (size_t)D * (size_t)(Nmax >> 1);
+    int dig_words = 0;
+    if (smem + cache <= (size_t)kFwdCacheBytes) {
+      smem += cache;
+      dig_words = D * (Nmax >> 1);
+    }
+    k_fwd2<D, false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf,
+                                                        dig_words);
   }
   return cudaGetLastError();
 }

@@ -45,6 +45,30 @@ def test_chunked_batch_matches_golden(small_chunks):
         assert PK.digest(c) == d[t], f"product {t}"
 
 
+def test_batch_timeline(gpu):
+    """The per-chunk timeline: host and device times in order, copies in
+    stream order, bytes summing to the batch's totals."""
+    _, triples = config3_head(48)
+    for chunk in (0, 20000):  # one chunk, then pipelined
+        api.set_chunk_limbs(chunk)
+        try:
+            api.matmul_batch(triples)
+        finally:
+            api.set_chunk_limbs(0)
+        st = api.batch_stats()
+        tl = api.batch_timeline()
+        assert len(tl) == st["chunks"]
+        assert (len(tl) == 1) == (chunk == 0)
+        assert sum(r["h2d_bytes"] for r in tl) == st["h2d_bytes"]
+        assert sum(r["d2h_bytes"] for r in tl) == st["d2h_bytes"]
+        for c, r in enumerate(tl):
+            assert 0 <= r["plan_begin"] <= r["plan_end"] <= r["queue_begin"] <= r["queue_end"]
+            assert 0 <= r["h2d_begin"] <= r["h2d_end"] <= r["kernels_end"] <= r["d2h_end"]
+            if c:
+                assert tl[c - 1]["h2d_end"] <= r["h2d_begin"]
+                assert tl[c - 1]["d2h_end"] <= r["d2h_end"]
+
+
 def test_pinned_batch_matches_golden(gpu):
     d = G.digests()["config3"]["C"]
     count = 64
