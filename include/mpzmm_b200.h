@@ -103,9 +103,9 @@ MPZMM_API int mpzmm_setup(int device);
    1 CUDA cores only, 2 tensor cores wherever the shape allows.
    The environment variable MPZMM_CONTRACT sets the initial value.
    MPZMM_OPT_CHUNK_LIMBS sets the input limbs per chunk of a pipelined
-   one-shot batch (mpzmm_matmul_batch): 0 (default) chooses an eighth of
-   the batch, at least 2^24 limbs; a batch no larger than one chunk runs
-   unchunked. */
+   one-shot batch (mpzmm_matmul_batch): 0 (default) chooses a 32nd of the
+   batch, kept between 2^22 and 2^26 limbs; a batch no larger than one
+   chunk runs unchunked. */
 #define MPZMM_OPT_CONTRACT 1
 #define MPZMM_OPT_CHUNK_LIMBS 2
 MPZMM_API int mpzmm_set_option(int option, int value);

@@ -24,15 +24,21 @@ cudaStream_t pick_stream(void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : context().stream;
 }
 
-int build_spec_packed(const mpzmm_product& p, ProductSpec* ps) {
+int check_product_packed(const mpzmm_product& p) {
   if (p.m < 0 || p.k < 0 || p.n < 0) return set_error(kErrArg, "negative dimension");
-  ps->m = p.m;
-  ps->k = p.k;
-  ps->n = p.n;
   const int64_t na = (int64_t)p.m * p.k, nb = (int64_t)p.k * p.n, nc = (int64_t)p.m * p.n;
   if ((na && (!p.a_offs || !p.a_sizes)) || (nb && (!p.b_offs || !p.b_sizes)) ||
       (nc && (!p.c_offs || !p.c_caps || !p.c_sizes || !p.c_limbs)))
     return set_error(kErrArg, "null array");
+  return kOk;
+}
+
+// the entry references of a checked product
+void fill_spec_packed(const mpzmm_product& p, ProductSpec* ps) {
+  ps->m = p.m;
+  ps->k = p.k;
+  ps->n = p.n;
+  const int64_t na = (int64_t)p.m * p.k, nb = (int64_t)p.k * p.n, nc = (int64_t)p.m * p.n;
   ps->a.resize(na);
   ps->b.resize(nb);
   ps->c.resize(nc);
@@ -46,6 +52,23 @@ int build_spec_packed(const mpzmm_product& p, ProductSpec* ps) {
   }
   for (int64_t e = 0; e < nc; ++e)
     ps->c[e] = OutRef{p.c_limbs + p.c_offs[e], p.c_caps[e], p.c_sizes + e, nullptr};
+}
+
+// All products checked (first error wins), then their references filled on
+// several host threads for a large batch.
+int build_specs_packed(int count, const mpzmm_product* products,
+                       std::vector<ProductSpec>* specs) {
+  uint64_t entries = 0;
+  for (int t = 0; t < count; ++t) {
+    const int st = check_product_packed(products[t]);
+    if (st) return st;
+    const mpzmm_product& p = products[t];
+    entries += (uint64_t)p.m * p.k + (uint64_t)p.k * p.n + (uint64_t)p.m * p.n;
+  }
+  specs->assign((size_t)count, ProductSpec());
+  parallel_chunks((size_t)count, (size_t)entries * 64, [&](size_t lo, size_t hi) {
+    for (size_t t = lo; t < hi; ++t) fill_spec_packed(products[t], &(*specs)[t]);
+  });
   return kOk;
 }
 
@@ -288,11 +311,9 @@ int mpzmm_matmul(int m, int k, int n, const uint64_t* a_limbs, const int64_t* a_
 
 int mpzmm_matmul_batch(int count, const mpzmm_product* products, void* stream) {
   if (count < 0 || (count > 0 && !products)) return set_error(kErrArg, "bad product list");
-  std::vector<ProductSpec> specs((size_t)count);
-  for (int t = 0; t < count; ++t) {
-    int st = build_spec_packed(products[t], &specs[t]);
-    if (st) return st;
-  }
+  std::vector<ProductSpec> specs;
+  const int st = build_specs_packed(count, products, &specs);
+  if (st) return st;
   return run_once(std::move(specs), stream);
 }
 
@@ -400,10 +421,8 @@ int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* product
   if (count < 0 || (count > 0 && !products)) return set_error(kErrArg, "bad product list");
   int st = ensure_setup(-1);
   if (st) return st;
-  std::vector<ProductSpec> specs((size_t)count);
-  for (int t = 0; t < count; ++t) {
-    if ((st = build_spec_packed(products[t], &specs[t]))) return st;
-  }
+  std::vector<ProductSpec> specs;
+  if ((st = build_specs_packed(count, products, &specs))) return st;
   std::unique_ptr<mpzmm_plan> p(new mpzmm_plan);
   if ((st = p->plan.build(std::move(specs)))) return st;
   if ((st = p->plan.upload(pick_stream(stream)))) return st;

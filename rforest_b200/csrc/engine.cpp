@@ -703,9 +703,20 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   };
   batch_classes(fwdg, true, fwd_groups_);
   batch_classes(invg, false, inv_groups_);
-  for (auto& kv : recg) {
-    Group g = std::move(kv.second);
-    g.max_r = (int)rec_min_r[g.P];  // narrowest r: sizes the CRT kernel's scratch
+  // CRT + recompose: the prime counts up to kCrtMixedSplit in one launch,
+  // the larger ones in another, each with its narrowest coefficient width
+  // per count (it sizes the kernel's scratch)
+  for (int high = 0; high < 2; ++high) {
+    Group g;
+    g.rmin.assign(kMaxPrimes + 1, 0);
+    for (auto& kv : recg) {
+      if ((kv.first > kCrtMixedSplit) != (high != 0)) continue;
+      g.rmin[kv.first] = (int)rec_min_r[kv.first];
+      g.P = std::max(g.P, kv.first);
+      g.idx.insert(g.idx.end(), kv.second.idx.begin(), kv.second.idx.end());
+    }
+    if (g.idx.empty()) continue;
+    g.crt_high = high != 0;
     // longest entries first (the warp that gets one works longest), ties in
     // entry order: one sort of packed (longest-first key, index) integers
     std::vector<uint64_t> keys(g.idx.size());
@@ -967,8 +978,8 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
   }
   if (timed) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
   for (const Group& g : rec_groups_)
-    CU(launch_crt_recompose(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, ws_->d_res,
-                            ws_->d_out, ws_->d_sizes, g.max_r, st),
+    CU(launch_crt_mixed(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.crt_high, g.rmin.data(),
+                        ws_->d_res, ws_->d_out, ws_->d_sizes, st),
        "CRT+recompose launch");
   if (timed) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
   return kOk;
@@ -1165,9 +1176,16 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   uint64_t total = 0;
   std::vector<uint64_t> limbs(specs.size());
   for (size_t t = 0; t < specs.size(); ++t) total += (limbs[t] = input_limbs(specs[t]));
-  // automatic chunks: an eighth of the batch, at least 16 Mi limbs (128 MB)
-  uint64_t chunk = ctx.chunk_limbs > 0 ? (uint64_t)ctx.chunk_limbs : total / 8;
-  if (ctx.chunk_limbs <= 0 && chunk < (16ull << 20)) chunk = 16ull << 20;
+  // automatic chunks: a 32nd of the batch, between 4 Mi and 64 Mi limbs (32
+  // and 512 MB of input) -- small enough that the first results come back
+  // early and both copy directions stream steadily, large enough that the
+  // kernels' launch tails stay small, bounded so that the workspaces in
+  // flight stay a few GB whatever the batch
+  uint64_t chunk = ctx.chunk_limbs > 0 ? (uint64_t)ctx.chunk_limbs : total / 32;
+  if (ctx.chunk_limbs <= 0) {
+    if (chunk < (4ull << 20)) chunk = 4ull << 20;
+    if (chunk > (64ull << 20)) chunk = 64ull << 20;
+  }
   if (chunk == 0) chunk = 1;
 
   if (specs.size() < 2 || total <= chunk) {

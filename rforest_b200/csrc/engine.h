@@ -257,6 +257,10 @@ class Plan {
     int max_lgN = 0;
     std::vector<CtaItem> items;
     uint32_t item_off = 0;
+    // CRT launch over several prime counts: the upper range, and the
+    // narrowest coefficient width per count
+    bool crt_high = false;
+    std::vector<int> rmin;
   };
 
   std::vector<ProductSpec> prods_;

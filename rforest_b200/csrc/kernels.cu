@@ -774,18 +774,15 @@ struct FastDiv {
   }
 };
 
+// One output entry by one warp: CRT of its coefficients tile by tile into
+// the warp's scratch sU (word q of tile coefficient c at [q * cmax + c]),
+// the words' sums, the carry ripple, the sign and the size.
 template <int P>
-__global__ void __launch_bounds__(32 * kCrtWarps)
-k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
-           const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
-           int32_t* __restrict__ out_sizes, int cmax) {
-  extern __shared__ uint32_t sm[];
+__device__ __forceinline__ void crt_entry(const InvDesc& d, const uint32_t* __restrict__ res,
+                                          uint32_t* __restrict__ out,
+                                          int32_t* __restrict__ out_sizes, uint32_t* sU,
+                                          int cmax, int lane) {
   const unsigned FULL = 0xffffffffu;
-  const int warp = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int slot = blockIdx.x * kCrtWarps + warp;
-  if (slot >= count) return;  // whole warp; no block-wide barrier below
-  const InvDesc d = descs[idx[slot]];
   // bit positions fit 31 bits (an entry's words times 32 stays below 2^31),
   // so index arithmetic is 32-bit and the divisions by r are multiply-highs
   const int r = (int)d.r;
@@ -793,7 +790,6 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
   const int W = (int)d.out_words;
   const int ncoef = (int)d.ncoef;
   uint32_t* o = out + d.out_word;
-  uint32_t* sU = sm + warp * (cmax * P);  // word q of tile coefficient c at [q * cmax + c]
 
   int hi_prev = 0, carry = 0;
   int first_nz = 0x7fffffff, last_nz = -1, last_no = -1;
@@ -904,6 +900,50 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
     const int limbs = top >= 0 ? top / 2 + 1 : 0;
     out_sizes[d.entry] = negative ? -limbs : limbs;
   }
+}
+
+// One prime count per launch.
+template <int P>
+__global__ void __launch_bounds__(32 * kCrtWarps)
+k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
+           const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
+           int32_t* __restrict__ out_sizes, int cmax) {
+  extern __shared__ uint32_t sm[];
+  const int warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kCrtWarps + warp;
+  if (slot >= count) return;  // whole warp; no block-wide barrier below
+  const InvDesc d = descs[idx[slot]];
+  crt_entry<P>(d, res, out, out_sizes, sm + warp * (cmax * P), cmax, threadIdx.x & 31);
+}
+
+template <int P, int PHI>
+__device__ __forceinline__ void crt_dispatch(const InvDesc& d, const uint32_t* __restrict__ res,
+                                             uint32_t* __restrict__ out,
+                                             int32_t* __restrict__ out_sizes, uint32_t* sU,
+                                             const CrtScratch& cs, int lane) {
+  if (d.P == P) {
+    crt_entry<P>(d, res, out, out_sizes, sU, cs.cmax[P], lane);
+  } else {
+    if constexpr (P < PHI) crt_dispatch<P + 1, PHI>(d, res, out, out_sizes, sU, cs, lane);
+  }
+}
+
+// Prime counts PLO..PHI in one launch (the entries longest first across
+// them, so the long entries of every count start together and the launch
+// has one tail instead of one per count); each warp's scratch holds
+// cs.warp_words words.
+template <int PLO, int PHI>
+__global__ void __launch_bounds__(32 * kCrtWarps)
+k_crt_mixed(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int count,
+            const uint32_t* __restrict__ res, uint32_t* __restrict__ out,
+            int32_t* __restrict__ out_sizes, CrtScratch cs) {
+  extern __shared__ uint32_t sm[];
+  const int warp = threadIdx.x >> 5;
+  const int slot = blockIdx.x * kCrtWarps + warp;
+  if (slot >= count) return;  // whole warp; no block-wide barrier below
+  const InvDesc d = descs[idx[slot]];
+  crt_dispatch<PLO, PHI>(d, res, out, out_sizes, sm + warp * cs.warp_words, cs,
+                         threadIdx.x & 31);
 }
 
 
@@ -1319,11 +1359,42 @@ cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items,
   return cudaGetLastError();
 }
 
+// coefficients a CRT tile can touch for coefficient width rmin
+static int crt_cmax(int P, int rmin) {
+  return (int)((32 * (int64_t)kCrtTileWords + 32 * P) / rmin + 3);
+}
+
+cudaError_t launch_crt_mixed(const InvDesc* descs, const uint32_t* idx, int count, bool high,
+                             const int* rmin, const uint32_t* res, uint32_t* out, int32_t* sizes,
+                             cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  const int plo = high ? kCrtMixedSplit + 1 : 2, phi = high ? kMaxPrimes : kCrtMixedSplit;
+  CrtScratch cs;
+  cs.warp_words = 0;
+  for (int P = 0; P <= kMaxPrimes; ++P) {
+    cs.cmax[P] = 0;
+    if (P < plo || P > phi || rmin[P] <= 0) continue;
+    cs.cmax[P] = crt_cmax(P, rmin[P]);
+    if (cs.cmax[P] * P > cs.warp_words) cs.warp_words = cs.cmax[P] * P;
+  }
+  if (cs.warp_words == 0) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(uint32_t) * (size_t)cs.warp_words * kCrtWarps;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  const int grid = (count + kCrtWarps - 1) / kCrtWarps;
+  if (high)
+    k_crt_mixed<kCrtMixedSplit + 1, kMaxPrimes><<<grid, 32 * kCrtWarps, smem, st>>>(
+        descs, idx, count, res, out, sizes, cs);
+  else
+    k_crt_mixed<2, kCrtMixedSplit><<<grid, 32 * kCrtWarps, smem, st>>>(descs, idx, count, res,
+                                                                      out, sizes, cs);
+  return cudaGetLastError();
+}
+
 template <int P>
 static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int count,
                                 const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
                                 cudaStream_t st) {
-  const int cmax = (int)((32 * (int64_t)kCrtTileWords + 32 * P) / rmin + 3);
+  const int cmax = crt_cmax(P, rmin);
   const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P);
   const size_t smem = per_warp * kCrtWarps;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
@@ -1409,6 +1480,13 @@ cudaError_t init_kernel_attributes() {
       (e = set_crt_attr<12>()) != cudaSuccess || (e = set_crt_attr<13>()) != cudaSuccess ||
       (e = set_crt_attr<14>()) != cudaSuccess || (e = set_crt_attr<15>()) != cudaSuccess ||
       (e = set_crt_attr<16>()) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_crt_mixed<2, kCrtMixedSplit>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
+          cudaSuccess ||
+      (e = cudaFuncSetAttribute(k_crt_mixed<kCrtMixedSplit + 1, kMaxPrimes>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
+          cudaSuccess)
     return e;
   return cudaFuncSetAttribute(k_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)((128 + 8 * tc::kMaxN) * 4 * tc::kMaxK));

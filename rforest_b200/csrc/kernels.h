@@ -61,4 +61,17 @@ cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int 
                                  const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
                                  cudaStream_t st);
 
+// The same over several prime counts in one launch: high = false takes the
+// entries with 2..kCrtMixedSplit primes, high = true those with more (each
+// launch's entries in idx, longest first); rmin[P] is the narrowest
+// coefficient width among the entries with P primes (0: none).
+constexpr int kCrtMixedSplit = 10;
+struct CrtScratch {
+  int cmax[kMaxPrimes + 1];  // tile coefficients per prime count
+  int warp_words;            // scratch words of one warp
+};
+cudaError_t launch_crt_mixed(const InvDesc* descs, const uint32_t* idx, int count, bool high,
+                             const int* rmin, const uint32_t* res, uint32_t* out, int32_t* sizes,
+                             cudaStream_t st);
+
 }  // namespace mpzmm

@@ -49,7 +49,7 @@ def test_batch_timeline(gpu):
     """The per-chunk timeline: host and device times in order, copies in
     stream order, bytes summing to the batch's totals."""
     _, triples = config3_head(48)
-    for chunk in (0, 20000):  # one chunk, then pipelined
+    for chunk in (1 << 30, 20000):  # one chunk, then pipelined
         api.set_chunk_limbs(chunk)
         try:
             api.matmul_batch(triples)
@@ -58,7 +58,7 @@ def test_batch_timeline(gpu):
         st = api.batch_stats()
         tl = api.batch_timeline()
         assert len(tl) == st["chunks"]
-        assert (len(tl) == 1) == (chunk == 0)
+        assert (len(tl) == 1) == (chunk == 1 << 30)
         assert sum(r["h2d_bytes"] for r in tl) == st["h2d_bytes"]
         assert sum(r["d2h_bytes"] for r in tl) == st["d2h_bytes"]
         for c, r in enumerate(tl):
@@ -75,7 +75,7 @@ def test_pinned_batch_matches_golden(gpu):
     _, triples = config3_head(count)
     b = api.Batch(triples, pinned=True)
     try:
-        for chunk in (0, 30000):  # unchunked, then pipelined
+        for chunk in (1 << 30, 30000):  # unchunked, then pipelined
             api.set_chunk_limbs(chunk)
             outs = b.run()
             st = api.batch_stats()
