@@ -425,7 +425,7 @@ def main():
         elif dom == 1:
             alg, t_ms, kern, stage = b2, stage_ms[1], "k_contract", "contract"
         else:
-            alg, t_ms, kern, stage = (b3, stage_ms[2] + stage_ms[3], "k_inv2+k_crt_warp",
+            alg, t_ms, kern, stage = (b3, stage_ms[2] + stage_ms[3], "k_inv2+k_crt_mixed",
                                       "inv_crt")
         # DRAM bytes per step of the stage on the 4096-product batch: ncu
         # (dram__bytes_read.sum + dram__bytes_write.sum) on the 512-product

@@ -1,14 +1,21 @@
 // sm_100a kernels of the exact matrix-product pipeline.
 //
-//   k_split_fwd      limbs -> r-bit coefficients -> residues mod p -> forward
-//                    NTT in shared memory (one CTA per (entry, prime))
+//   k_fwd2           limbs -> r-bit coefficients -> 30-bit digits ->
+//                    residues mod p -> forward NTT, register-blocked passes
+//                    (several small transforms or one large one per CTA)
+//   k_split_fwd      the same, radix 2, one CTA per (entry, prime): tiny
+//                    transforms and digit counts above 7
 //   k_contract       per frequency h and prime: C[h] = A[h] B[h] mod p on
 //                    CUDA cores (64-bit lazy accumulation, Montgomery fold)
-//   k_inv_ntt        inverse NTT in shared memory (one CTA per (entry, prime))
-//   k_crt_warp       explicit CRT to signed multi-word coefficients, then
+//   k_contract_tc    the same on tensor cores (tcgen05 kind::i8, exact
+//                    byte split; contract_tc.cuh)
+//   k_inv2           inverse NTT, register-blocked; k_inv_ntt radix 2
+//   k_crt_mixed      explicit CRT to signed multi-word coefficients, then
 //                    sum_i c_i 2^(i r) with carries resolved by a
 //                    carry-lookahead prefix scan over 32-bit output words,
-//                    sign + negation + normalisation (one warp per entry)
+//                    sign + negation + normalisation (one warp per entry,
+//                    every prime count of a range in one launch);
+//                    k_crt_warp the same for one prime count
 //
 // Reference counterparts: split/reduce src/lib/split_reduce.c:15-66,
 // NTTs src/lib/mpnfft.c:354-432, contraction src/lib/mpnfft.c:559-651,
