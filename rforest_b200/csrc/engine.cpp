@@ -238,6 +238,7 @@ void teardown() {
     if (g_ctx.pipe_ev) cudaEventDestroy(g_ctx.pipe_ev);
     for (auto* v : {&g_ctx.pipe_ev_in, &g_ctx.pipe_ev_exec, &g_ctx.pipe_ev_out})
       for (cudaEvent_t e : *v) cudaEventDestroy(e);
+    for (cudaEvent_t e : g_ctx.tl_ev) cudaEventDestroy(e);
     delete g_ctx.ws;
   }
   cudaStreamDestroy(g_ctx.stream);
