@@ -141,6 +141,14 @@ MPZMM_API int mpzmm_batch_stats(int64_t *ns4, int64_t *chunks, int64_t *bytes4);
 #define MPZMM_TIMELINE_FIELDS 10
 MPZMM_API int mpzmm_batch_timeline(double *rows, int max_chunks, int *nchunks);
 
+/* How mpzmm_matmul_batch would split a batch whose products have limbs[t]
+   input limbs each (A's and B's limbs together), with chunk_limbs as
+   MPZMM_OPT_CHUNK_LIMBS (0: automatic): *nchunks gets the chunk count and
+   bounds (may be NULL; up to max_bounds values) the product index where
+   each chunk starts, then the count.  Host only; no device needed. */
+MPZMM_API int mpzmm_batch_chunks(int count, const int64_t *limbs, int64_t chunk_limbs,
+                                 int64_t *bounds, int max_bounds, int *nchunks);
+
 /* Autotuner: times the contraction of a representative product per size
    class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
    entries) on CUDA cores and on tensor cores and makes automatic mode use

@@ -114,6 +114,8 @@ def lib():
         "mpzmm_host_unregister": (C.c_int, [vp]),
         "mpzmm_batch_stats": (C.c_int, [i64p, i64p, i64p]),
         "mpzmm_batch_timeline": (C.c_int, [C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
+        "mpzmm_batch_chunks": (C.c_int, [C.c_int, i64p, C.c_int64, i64p, C.c_int,
+                                         C.POINTER(C.c_int)]),
         "mpzmm_chain_output_limbs": (C.c_int64, [C.c_int, C.POINTER(Matrix)]),
         "mpzmm_chain": (C.c_int, [C.c_int, C.POINTER(Matrix), u64p, i64p, i64p, i32p, vp]),
         "mpzmm_mod_create": (C.c_int, [C.POINTER(vp), u64p, C.c_int32, C.c_int64]),

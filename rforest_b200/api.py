@@ -92,6 +92,19 @@ def batch_timeline():
     return [dict(zip(TIMELINE_FIELDS, rows[c * F:(c + 1) * F])) for c in range(n.value)]
 
 
+def batch_chunks(limbs: Sequence[int], chunk_limbs: int = 0) -> List[int]:
+    """Product-index bounds of the chunks mpzmm_matmul_batch would use for
+    products with these input limb counts (chunk_limbs 0: automatic); the
+    last bound is the product count."""
+    arr = np.ascontiguousarray(np.asarray(limbs, dtype=np.int64).reshape(-1))
+    n = C.c_int()
+    bounds = np.zeros(arr.size + 2, dtype=np.int64)
+    _lib.check(_lib.lib().mpzmm_batch_chunks(
+        int(arr.size), arr.ctypes.data_as(C.POINTER(C.c_int64)), int(chunk_limbs),
+        bounds.ctypes.data_as(C.POINTER(C.c_int64)), int(bounds.size), C.byref(n)))
+    return [int(b) for b in bounds[:n.value + 1]]
+
+
 class HostArena:
     """Pinned host memory from the library (mpzmm_host_alloc).  Transfers
     whose host side lies inside it go straight to and from the device."""

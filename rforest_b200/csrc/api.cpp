@@ -220,6 +220,23 @@ int mpzmm_batch_stats(int64_t* ns4, int64_t* chunks, int64_t* bytes4) {
   return kOk;
 }
 
+int mpzmm_batch_chunks(int count, const int64_t* limbs, int64_t chunk_limbs, int64_t* bounds,
+                       int max_bounds, int* nchunks) {
+  if (count < 0 || (count > 0 && !limbs)) return set_error(kErrArg, "bad limb counts");
+  std::vector<uint64_t> l((size_t)count);
+  for (int t = 0; t < count; ++t) {
+    if (limbs[t] < 0) return set_error(kErrArg, "negative limb count");
+    l[t] = (uint64_t)limbs[t];
+  }
+  std::vector<size_t> b;
+  batch_chunks(l, chunk_limbs, &b);
+  const int n = (int)b.size() - 1;
+  if (nchunks) *nchunks = n;
+  if (bounds)
+    for (int i = 0; i <= n && i < max_bounds; ++i) bounds[i] = (int64_t)b[i];
+  return kOk;
+}
+
 static_assert(MPZMM_TIMELINE_FIELDS == mpzmm::kTimelineFields, "timeline row size");
 
 int mpzmm_batch_timeline(double* rows, int max_chunks, int* nchunks) {

@@ -1164,6 +1164,57 @@ void read_timeline(Context& ctx, size_t nchunks) {
 }
 }  // namespace
 
+bool batch_chunks(const std::vector<uint64_t>& limbs, int64_t chunk_option,
+                  std::vector<size_t>* bounds) {
+  const size_t n = limbs.size();
+  uint64_t total = 0;
+  for (uint64_t l : limbs) total += l;
+  // automatic chunks: a 32nd of the batch, between 4 Mi and 64 Mi limbs (32
+  // and 512 MB of input) -- small enough that the first results come back
+  // early and both copy directions stream steadily, large enough that the
+  // kernels' launch tails stay small, bounded so that the workspaces in
+  // flight stay a few GB whatever the batch
+  uint64_t chunk = chunk_option > 0 ? (uint64_t)chunk_option : total / 32;
+  if (chunk_option <= 0) {
+    if (chunk < (4ull << 20)) chunk = 4ull << 20;
+    if (chunk > (64ull << 20)) chunk = 64ull << 20;
+  }
+  if (chunk == 0) chunk = 1;
+  bounds->assign(1, 0);
+  if (n < 2 || total <= chunk) {
+    bounds->push_back(n);
+    return false;
+  }
+  // chunks of consecutive whole products; the first two are a quarter and
+  // a half of the others, so the first results start back sooner (the
+  // device->host copies are the pipeline's longest chain),
+  uint64_t acc = 0;
+  for (size_t t = 0; t < n; ++t) {
+    acc += limbs[t];
+    const size_t c = bounds->size() - 1;
+    const uint64_t target = c == 0 ? chunk / 4 : (c == 1 ? chunk / 2 : chunk);
+    if (acc >= target && t + 1 < n) {
+      bounds->push_back(t + 1);
+      acc = 0;
+    }
+  }
+  bounds->push_back(n);
+  // and the last one is split about 2:1, so the final results come back
+  // sooner after the last inputs went in
+  if (bounds->size() >= 3) {
+    const size_t a = (*bounds)[bounds->size() - 2], b = bounds->back();
+    uint64_t tail = 0;
+    for (size_t t = a; t < b; ++t) tail += limbs[t];
+    if (tail > chunk / 2 && b - a >= 2) {
+      uint64_t acc2 = 0;
+      size_t cut = a;
+      while (cut + 1 < b && 3 * (acc2 + limbs[cut]) <= 2 * tail) acc2 += limbs[cut++];
+      if (cut > a) bounds->insert(bounds->end() - 1, cut);
+    }
+  }
+  return true;
+}
+
 int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   Context& ctx = context();
   for (auto& v : ctx.batch_ns) v = 0;
@@ -1174,22 +1225,12 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     ctx.batch_bytes[2] += (int64_t)p.direct_in_bytes();
     ctx.batch_bytes[3] += (int64_t)p.direct_out_bytes();
   };
-  uint64_t total = 0;
   std::vector<uint64_t> limbs(specs.size());
-  for (size_t t = 0; t < specs.size(); ++t) total += (limbs[t] = input_limbs(specs[t]));
-  // automatic chunks: a 32nd of the batch, between 4 Mi and 64 Mi limbs (32
-  // and 512 MB of input) -- small enough that the first results come back
-  // early and both copy directions stream steadily, large enough that the
-  // kernels' launch tails stay small, bounded so that the workspaces in
-  // flight stay a few GB whatever the batch
-  uint64_t chunk = ctx.chunk_limbs > 0 ? (uint64_t)ctx.chunk_limbs : total / 32;
-  if (ctx.chunk_limbs <= 0) {
-    if (chunk < (4ull << 20)) chunk = 4ull << 20;
-    if (chunk > (64ull << 20)) chunk = 64ull << 20;
-  }
-  if (chunk == 0) chunk = 1;
+  for (size_t t = 0; t < specs.size(); ++t) limbs[t] = input_limbs(specs[t]);
+  std::vector<size_t> bounds;
+  const bool pipelined = batch_chunks(limbs, ctx.chunk_limbs, &bounds);
 
-  if (specs.size() < 2 || total <= chunk) {
+  if (!pipelined) {
     ctx.batch_chunks = 1;
     int s = ensure_timeline(ctx, 1);
     if (s) return s;
@@ -1228,34 +1269,6 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     return s;
   }
 
-  // chunks of consecutive whole products; the first two are a quarter and
-  // a half of the others, so the first results start back sooner (the
-  // device->host copies are the pipeline's longest chain),
-  std::vector<size_t> bounds{0};
-  uint64_t acc = 0;
-  for (size_t t = 0; t < specs.size(); ++t) {
-    acc += limbs[t];
-    const size_t c = bounds.size() - 1;
-    const uint64_t target = c == 0 ? chunk / 4 : (c == 1 ? chunk / 2 : chunk);
-    if (acc >= target && t + 1 < specs.size()) {
-      bounds.push_back(t + 1);
-      acc = 0;
-    }
-  }
-  bounds.push_back(specs.size());
-  // and the last one is split about 2:1, so the final results come back
-  // sooner after the last inputs went in
-  if (bounds.size() >= 3) {
-    const size_t a = bounds[bounds.size() - 2], b = bounds.back();
-    uint64_t tail = 0;
-    for (size_t t = a; t < b; ++t) tail += limbs[t];
-    if (tail > chunk / 2 && b - a >= 2) {
-      uint64_t acc2 = 0;
-      size_t cut = a;
-      while (cut + 1 < b && 3 * (acc2 + limbs[cut]) <= 2 * tail) acc2 += limbs[cut++];
-      if (cut > a) bounds.insert(bounds.end() - 1, cut);
-    }
-  }
   const size_t nchunks = bounds.size() - 1;
   ctx.batch_chunks = (int64_t)nchunks;
   int s = ensure_pipeline(ctx);

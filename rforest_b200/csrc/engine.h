@@ -342,6 +342,11 @@ class Plan {
 // their results (two copy streams also keep the copy directions on
 // separate copy queues).  Returns when every result is written.
 int run_batch(std::vector<ProductSpec> specs, cudaStream_t st);
+// How run_batch splits a batch whose products have `limbs` input limbs each
+// (chunk_option: MPZMM_OPT_CHUNK_LIMBS, 0 automatic): product-index bounds
+// (first 0, last the count); false when it runs as one unchunked pass.
+bool batch_chunks(const std::vector<uint64_t>& limbs, int64_t chunk_option,
+                  std::vector<size_t>* bounds);
 
 // Chain of products, each step's A being the previous step's result kept in
 // device memory (steps[0] is an ordinary product; steps[i > 0] give B and
