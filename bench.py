@@ -24,6 +24,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -151,11 +152,10 @@ class ClockSampler:
 
     def __init__(self, device_index: int):
         self.proc = None
-        self.path = os.path.join(ROOT, "_work", f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mpzmm_clocks_{os.getpid()}.csv")
         self.dev = device_index
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(

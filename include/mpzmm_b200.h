@@ -76,13 +76,18 @@ MPZMM_API void cu_mpz_rmatrix_mult_fft(mpz_t *C, mpz_t *A, int r, mpz_t *B, int 
    src/lib/hwmpz.c:249-255): 1 if this library can multiply these operands. */
 MPZMM_API int mpz_rmatrix_gpu_fft_suitable(mpz_t *A, int r, mpz_t *B, int d);
 
-/* src/include/hwmpz.h:130 and :134 (header inlines in the reference). */
+/* src/include/hwmpz.h:130 and :134 (header inlines in the reference).  A
+   caller that also includes the reference's own hwmpz.h first (whose guard is
+   _HWMPZ_INCLUDE_) keeps that header's definitions of these two wrappers;
+   the declarations above are then checked against it by the compiler. */
+#ifndef _HWMPZ_INCLUDE_
 static inline void mpz_matrix_mult_fft(mpz_t *C, mpz_t *A, mpz_t *B, int d, mpz_t w) {
   mpz_rmatrix_mult_fft(C, A, d, B, d, w);
 }
 static inline void cu_mpz_matrix_mult_fft(mpz_t *C, mpz_t *A, mpz_t *B, int d, mpz_t w) {
   cu_mpz_rmatrix_mult_fft(C, A, d, B, d, w);
 }
+#endif
 
 /* Fatal-error hook for the void entry points above (default: print the
    error to stderr and abort()).  No counterpart in the reference. */
@@ -108,6 +113,16 @@ MPZMM_API int mpzmm_setup(int device);
    chunk runs unchunked. */
 #define MPZMM_OPT_CONTRACT 1
 #define MPZMM_OPT_CHUNK_LIMBS 2
+/* Failure injection, for tests of a caller's error handling (no counterpart
+   in the reference; nothing here faults a GPU).  MPZMM_OPT_TEST_STALL_TC:
+   the next `value` tensor-core contraction launches issue no tensor work,
+   so each of their CTAs' bounded waits (one second) runs out and the call
+   returns MPZMM_ERR_TIMEOUT; the context stays usable.
+   MPZMM_OPT_TEST_FAIL_ALLOC: the next `value` device or pinned-host
+   allocations of a workspace fail as if out of memory (MPZMM_ERR_NOMEM).
+   Reading either option returns the injections still pending. */
+#define MPZMM_OPT_TEST_STALL_TC 100
+#define MPZMM_OPT_TEST_FAIL_ALLOC 101
 MPZMM_API int mpzmm_set_option(int option, int value);
 MPZMM_API int mpzmm_get_option(int option);
 
@@ -304,8 +319,11 @@ MPZMM_API int mpzmm_plan_info(const mpzmm_plan *plan, int64_t *launches_per_exec
    than 2^15 points, are rejected with MPZMM_ERR_TOO_LARGE.  The first call
    on a device sets up that device's tables (make it before any stream
    capture).  All calls share the one scratch array and leave their data in
-   it: calls whose GPU work overlaps race, so serialise them.  Asynchronous
-   on `stream` (NULL: the legacy default stream). */
+   it: calls whose GPU work overlaps race, so serialise them.  Nothing of
+   the caller's is touched when a call is refused.  The kernels run
+   asynchronously on `stream` (NULL: the legacy default stream); the call
+   itself returns once its descriptors have been copied from the library's
+   pageable host buffer, which CUDA stages after the stream's earlier work. */
 MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
                                    const uint64_t *d_a_limbs, const int64_t *a_offs,
                                    const int32_t *a_sizes,

@@ -31,13 +31,24 @@ _MATMUL_ARGS = [C.c_int, C.c_int, C.c_int, _u64p, _i64p, _i32p, _u64p, _i64p,
 _oracle = None
 _ref = None
 
+# Where the reference source tree lies (read only while building oracle/_ref;
+# nothing reads it at run time).  RFOREST_REFERENCE overrides the default.
+REFERENCE_DIR = os.environ.get("RFOREST_REFERENCE", "/root/reference")
+
+
+def reference_tree_present() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE_DIR, "src", "lib"))
+
 
 def build(with_reference: bool = True) -> None:
     """Compile the oracle (and, where the reference tree exists, oracle/_ref)."""
     targets = ["oracle"]
-    if with_reference and os.path.isdir("/root/reference/src/lib"):
+    if with_reference and reference_tree_present():
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+        # the reference's own drivers linked against the product library
+        if os.path.exists(os.path.join(HERE, "..", "rforest_b200", "lib", "libmpzmm_b200.so")):
+            targets.append("dropin")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_DIR}"] + targets, check=True)
 
 
 def _load_oracle():

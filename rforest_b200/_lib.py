@@ -21,6 +21,8 @@ MPZMM_ERR_BUSY = 8
 
 MPZMM_OPT_CONTRACT = 1
 MPZMM_OPT_CHUNK_LIMBS = 2
+MPZMM_OPT_TEST_STALL_TC = 100
+MPZMM_OPT_TEST_FAIL_ALLOC = 101
 CONTRACT_AUTO, CONTRACT_CUDA_CORES, CONTRACT_TENSOR_CORES = 0, 1, 2
 
 u64p = C.POINTER(C.c_uint64)

@@ -123,6 +123,16 @@ int mpzmm_set_option(int option, int value) {
     context().chunk_limbs = value;
     return kOk;
   }
+  if (option == MPZMM_OPT_TEST_STALL_TC) {
+    if (value < 0) return set_error(kErrArg, "count must be >= 0");
+    set_test_stall_tc(value);
+    return kOk;
+  }
+  if (option == MPZMM_OPT_TEST_FAIL_ALLOC) {
+    if (value < 0) return set_error(kErrArg, "count must be >= 0");
+    set_test_fail_alloc(value);
+    return kOk;
+  }
   return set_error(kErrArg, "unknown option");
 }
 
@@ -202,6 +212,8 @@ int mpzmm_autotune(void* stream, float* ms_out) {
 int mpzmm_get_option(int option) {
   if (option == MPZMM_OPT_CONTRACT) return context().contract_mode;
   if (option == MPZMM_OPT_CHUNK_LIMBS) return (int)context().chunk_limbs;
+  if (option == MPZMM_OPT_TEST_STALL_TC) return test_stall_tc();
+  if (option == MPZMM_OPT_TEST_FAIL_ALLOC) return test_fail_alloc();
   return -1;
 }
 

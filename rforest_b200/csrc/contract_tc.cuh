@@ -21,8 +21,9 @@
 // K-major no-swizzle layout (8-row x 16-byte core matrices), one elected
 // thread issues the MMAs (M = 128 rows = TMEM lanes, N <= 256 per MMA,
 // K = 32 bytes per MMA), tcgen05.commit arrives on an mbarrier, and warp w
-// reads TMEM lanes 32w..32w+31.  Every wait is bounded: on time-out the CTA
-// records an error, stops issuing work, frees its TMEM and returns.
+// reads TMEM lanes 32w..32w+31.  Every wait is bounded (one second of wall
+// time): on time-out the CTA records an error, stops issuing work, frees its
+// TMEM and returns.
 #pragma once
 
 #include <cstdint>
@@ -36,6 +37,7 @@ constexpr int kMaxN = 64;        // n <= 64  -> 8n <= 512 TMEM columns
 constexpr int kMaxM = 128;       // one M = 128 tile
 constexpr int kTmemCols = 512;   // allocated per CTA (one CTA per SM by shared memory)
 constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // one second of wall time
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -75,7 +77,16 @@ __device__ __forceinline__ uint32_t split_bytes(uint32_t x, uint32_t p) {
   return packed;
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase with the given parity to complete; gives up (false)
+// after kWaitLimitNs of wall time or kSpinLimit polls, whichever comes first.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  uint64_t t0 = 0;
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
     uint32_t done;
     asm volatile(
@@ -86,6 +97,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
         : "r"(bar), "r"(phase)
         : "memory");
     if (done) return true;
+    if ((it & 63u) == 0) {
+      const uint64_t t = global_ns();
+      if (it == 0)
+        t0 = t;
+      else if (t - t0 > kWaitLimitNs)
+        return false;
+    }
   }
   return false;
 }

@@ -2,6 +2,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -58,6 +59,24 @@ int set_error(int status, const std::string& msg) {
 const char* last_error() { return g_err.c_str(); }
 
 Context& context() { return g_ctx; }
+
+namespace {
+std::atomic<int> g_test_stall_tc{0};
+std::atomic<int> g_test_fail_alloc{0};
+bool take_one(std::atomic<int>& c) {
+  int v = c.load();
+  while (v > 0)
+    if (c.compare_exchange_weak(v, v - 1)) return true;
+  return false;
+}
+}  // namespace
+
+void set_test_stall_tc(int count) { g_test_stall_tc = count > 0 ? count : 0; }
+void set_test_fail_alloc(int count) { g_test_fail_alloc = count > 0 ? count : 0; }
+int test_stall_tc() { return g_test_stall_tc.load(); }
+int test_fail_alloc() { return g_test_fail_alloc.load(); }
+bool take_test_stall_tc() { return take_one(g_test_stall_tc); }
+bool take_test_fail_alloc() { return take_one(g_test_fail_alloc); }
 
 std::mutex& workspace_mutex() {
   static std::mutex mu;
@@ -287,6 +306,8 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
     }
     *p = nullptr;
     cap = 0;
+    if (take_test_fail_alloc())
+      return set_error(kErrNoMem, "injected device allocation failure (test option)");
     auto alloc = [&](size_t count) {
       return async_stream ? cudaMallocAsync((void**)p, count * elem, async_stream)
                           : cudaMalloc((void**)p, count * elem);
@@ -313,6 +334,8 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
     if (*p) cudaFreeHost(*p);
     *p = nullptr;
     cap = 0;
+    if (take_test_fail_alloc())
+      return set_error(kErrNoMem, "injected pinned-host allocation failure (test option)");
     cudaError_t e = cudaMallocHost((void**)p, want * elem);
     if (e != cudaSuccess) {
       *p = nullptr;
@@ -964,7 +987,7 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
   if (!tc_items_.empty())
     CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, kTcFreqsPerCta,
-                          tc_max_k_, tc_max_n_, ws_->d_status, st),
+                          tc_max_k_, tc_max_n_, ws_->d_status, st, take_test_stall_tc() ? 1 : 0),
        "tensor-core contraction launch");
   if (timed) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
   for (const Group& g : inv_groups_) {

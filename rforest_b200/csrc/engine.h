@@ -179,6 +179,19 @@ constexpr int kTcFreqsPerCta = 16;
 Context& context();
 std::mutex& workspace_mutex();
 
+// Failure injection for the library's own failure-path tests (host side
+// only; nothing faults a GPU): the next `count` tensor-core contraction
+// launches issue no tensor work, so their bounded waits run out
+// (MPZMM_ERR_TIMEOUT); the next `count` device or pinned-host allocations
+// of a workspace report failure (MPZMM_ERR_NOMEM).
+void set_test_stall_tc(int count);
+void set_test_fail_alloc(int count);
+int test_stall_tc();
+int test_fail_alloc();
+// consumes one pending injection (true if one was pending)
+bool take_test_stall_tc();
+bool take_test_fail_alloc();
+
 // Runs fn(lo, hi) over [0, n) split across host threads when `bytes` is
 // large enough to be worth it (gather/scatter of limbs).
 void parallel_chunks(size_t n, size_t bytes, const std::function<void(size_t, size_t)>& fn);

@@ -959,7 +959,7 @@ k_crt_mixed(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(tc::kThreads, 1)
 k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
-              uint32_t* __restrict__ res, int fb, int* __restrict__ status) {
+              uint32_t* __restrict__ res, int fb, int* __restrict__ status, int stall) {
   extern __shared__ __align__(1024) uint8_t tsm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tmem_slot;
@@ -1025,7 +1025,10 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0) {
+    // stall (failure-path tests only): no MMA and no commit are issued, so
+    // nothing ever arrives on the barrier and the bounded wait below runs out
+    // with no tensor operation outstanding
+    if (tid == 0 && !stall) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (uint32_t t0 = 0; t0 < ncols; t0 += 256) {
         const uint32_t nt = (ncols - t0) < 256u ? (ncols - t0) : 256u;
@@ -1355,14 +1358,14 @@ bool contract_tc_eligible(int m, int k, int n) {
 
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
                                uint32_t* res, int fb, int max_k, int max_n, int* status,
-                               cudaStream_t st) {
+                               cudaStream_t st, int stall) {
   if (count == 0) return cudaSuccess;
   const size_t kprime = (size_t)((4 * max_k + 31) & ~31);
   const size_t ncols = (size_t)((8 * max_n + 15) & ~15);
   size_t smem = (128 + ncols) * kprime;
   // at least 120 KB so that one CTA (512 TMEM columns) runs per SM
   if (smem < 120 * 1024) smem = 120 * 1024;
-  k_contract_tc<<<count, tc::kThreads, smem, st>>>(prods, items, res, fb, status);
+  k_contract_tc<<<count, tc::kThreads, smem, st>>>(prods, items, res, fb, status, stall);
   return cudaGetLastError();
 }
 

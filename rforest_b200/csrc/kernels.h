@@ -49,11 +49,12 @@ cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_
 
 // Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
 // k <= 64, n <= 64; each work item covers `fb` consecutive frequencies.
-// *status is set to 1 if a bounded wait gave up.
+// *status is set to 1 if a bounded wait gave up.  stall != 0 (failure-path
+// tests only) issues no tensor work, so every CTA's wait runs out.
 bool contract_tc_eligible(int m, int k, int n);
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
                                uint32_t* res, int fb, int max_k, int max_n, int* status,
-                               cudaStream_t st);
+                               cudaStream_t st, int stall = 0);
 
 // CRT + recompose + sign for `count` output entries with P primes; rmin is
 // the narrowest coefficient width among them (it sizes the shared scratch).

@@ -107,6 +107,9 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   if ((na && (!a_offs || !a_sizes || !d_a_limbs)) || (nb && (!b_offs || !b_sizes || !d_b_limbs)) ||
       !c_offs || !c_caps || !d_c_sizes || !d_c_limbs)
     return set_error(kErrArg, "null array");
+  // the product descriptor holds the dimensions in 16 bits
+  if (m > 65535 || k > 65535 || n > 65535)
+    return set_error(kErrTooLarge, "mpzmm_matmul_noalloc: dimension > 65535");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cufail(e, "cudaGetDevice");
@@ -114,10 +117,6 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   int st = setup_device(dev, &ds);
   if (st) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-
-  // results start cleared: every size is rewritten below or stays 0
-  if ((e = cudaMemsetAsync(d_c_sizes, 0, sizeof(int32_t) * (size_t)nc, s)) != cudaSuccess)
-    return cufail(e, "cudaMemsetAsync(sizes)");
 
   // operand bit lengths bounded from the limb counts (the limbs are on the device)
   int64_t a_bits = 0, b_bits = 0;
@@ -132,7 +131,11 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   Params prm;
   if (!choose_params(a_bits, b_bits, m, k, n, &prm))
     return set_error(kErrTooLarge, "mpzmm_matmul_noalloc: product too large");
-  if (prm.P == 0) return kOk;  // identically zero: sizes already cleared
+  if (prm.P == 0) {  // identically zero: every result size is 0
+    if ((e = cudaMemsetAsync(d_c_sizes, 0, sizeof(int32_t) * (size_t)nc, s)) != cudaSuccess)
+      return cufail(e, "cudaMemsetAsync(sizes)");
+    return kOk;
+  }
   if (prm.lgN > kNoAllocLgN)
     return set_error(kErrTooLarge, "mpzmm_matmul_noalloc: transform of 2^" +
                                        std::to_string(prm.lgN) + " points exceeds the 2^" +
@@ -216,6 +219,13 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   }
   uint8_t* dd = ds->scratch;
   uint32_t* dres = reinterpret_cast<uint32_t*>(ds->scratch + desc_bytes);
+  // every check has passed: only now is anything of the caller's touched.
+  // Results start cleared: every size is rewritten by the CRT kernel or
+  // stays 0.
+  if ((e = cudaMemsetAsync(d_c_sizes, 0, sizeof(int32_t) * (size_t)nc, s)) != cudaSuccess)
+    return cufail(e, "cudaMemsetAsync(sizes)");
+  // a copy from pageable memory: it returns once the descriptors are staged,
+  // so the next call may reuse g_host_desc
   if ((e = cudaMemcpyAsync(dd, hd, desc_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cufail(e, "descriptor upload");
   const FwdDesc* dfwd = reinterpret_cast<const FwdDesc*>(dd + off_fwd);

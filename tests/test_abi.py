@@ -107,3 +107,34 @@ def test_mpz_array_roundtrip():
     a = gmp.MpzArray(vals)
     assert a.to_ints() == vals
     a.close()
+
+
+def test_failure_injection_options_host_only(product_lib):
+    """The failure-injection options are host state: set, read back, rejected
+    when negative, cleared (no device needed)."""
+    L = product_lib
+    for opt in (_lib.MPZMM_OPT_TEST_STALL_TC, _lib.MPZMM_OPT_TEST_FAIL_ALLOC):
+        assert L.mpzmm_set_option(opt, 3) == _lib.MPZMM_OK
+        assert L.mpzmm_get_option(opt) == 3
+        assert L.mpzmm_set_option(opt, -1) == _lib.MPZMM_ERR_ARG
+        assert L.mpzmm_set_option(opt, 0) == _lib.MPZMM_OK
+        assert L.mpzmm_get_option(opt) == 0
+
+
+def test_reference_drivers_link_against_the_library():
+    """Where the reference tree exists, its own tests/test_matmul.c and
+    benchmark/bench_matmul.c compile unmodified with this library's header
+    forced in after the reference's (a declaration mismatch would fail the
+    compile) and resolve libmpzmm_b200.so at load time."""
+    import subprocess
+    from oracle import oracle as O
+    if not O.reference_tree_present():
+        pytest.skip("reference tree not present")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run(["make", "-s", "-C", os.path.join(root, "oracle"),
+                    f"REF={O.REFERENCE_DIR}", "dropin"], check=True)
+    for exe in ("test_matmul_b200", "bench_matmul_b200"):
+        path = os.path.join(root, "oracle", "_ref", exe)
+        out = subprocess.run(["ldd", path], capture_output=True, text=True, check=True).stdout
+        line = [ln for ln in out.splitlines() if "libmpzmm_b200.so" in ln]
+        assert line and "not found" not in line[0], out

@@ -77,3 +77,57 @@ def test_noalloc_rejects_oversize(product_lib):
         _noalloc(16, 16, 16, A, B)
     assert e.value.status == _lib.MPZMM_ERR_TOO_LARGE
     assert "scratch" in str(e.value) or "limit" in str(e.value)
+
+
+def _noalloc_raw(m, k, n, A: PK.Packed, B: PK.Packed, cap_delta=0):
+    """One call with explicit capacities (the bound plus cap_delta); returns
+    (status, result sizes on the device after the call)."""
+    import torch
+    L = _lib.lib()
+    cap = api.output_limbs(k, 64 * A.max_limbs(), 64 * B.max_limbs()) + cap_delta
+    dev = torch.device("cuda", 0)
+    d_a = torch.from_numpy(np.ascontiguousarray(A.limbs, dtype=np.uint64).view(np.int64)).to(dev)
+    d_b = torch.from_numpy(np.ascontiguousarray(B.limbs, dtype=np.uint64).view(np.int64)).to(dev)
+    d_c = torch.zeros(m * n * max(cap, 1), dtype=torch.int64, device=dev)
+    d_sz = torch.full((m * n,), 777, dtype=torch.int32, device=dev)
+    c_offs = np.arange(m * n, dtype=np.int64) * max(cap, 1)
+    c_caps = np.full(m * n, cap, dtype=np.int64)
+    a_offs = np.ascontiguousarray(A.offs, dtype=np.int64)
+    a_sz = np.ascontiguousarray(A.sizes, dtype=np.int32)
+    b_offs = np.ascontiguousarray(B.offs, dtype=np.int64)
+    b_sz = np.ascontiguousarray(B.sizes, dtype=np.int32)
+    stream = torch.cuda.current_stream(dev)
+    st = L.mpzmm_matmul_noalloc(
+        m, k, n, C.c_void_p(d_a.data_ptr()), a_offs.ctypes.data_as(_lib.i64p),
+        a_sz.ctypes.data_as(_lib.i32p), C.c_void_p(d_b.data_ptr()),
+        b_offs.ctypes.data_as(_lib.i64p), b_sz.ctypes.data_as(_lib.i32p),
+        C.c_void_p(d_c.data_ptr()), c_offs.ctypes.data_as(_lib.i64p),
+        c_caps.ctypes.data_as(_lib.i64p), C.c_void_p(d_sz.data_ptr()),
+        C.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize(dev)
+    return st, d_sz.cpu().numpy().tolist()
+
+
+def test_noalloc_rejects_long_transform_untouched(product_lib):
+    """Few entries but a transform above 2^15 points: refused with
+    MPZMM_ERR_TOO_LARGE, and the caller's result sizes are left as they were."""
+    A = PK.from_ints([(1 << (1 << 22)) - 5])
+    B = PK.from_ints([-((1 << (1 << 22)) - 7)])
+    st, sizes = _noalloc_raw(1, 1, 1, A, B)
+    assert st == _lib.MPZMM_ERR_TOO_LARGE
+    msg = _lib.lib().mpzmm_last_error().decode()
+    assert "2^15" in msg or "too large" in msg
+    assert sizes == [777]
+
+
+def test_noalloc_rejects_short_capacity_untouched(product_lib):
+    """One limb short of the stated capacity: MPZMM_ERR_CAPACITY, nothing run."""
+    A = PK.from_ints([(1 << 1000) + 1, 3, -5, 7])
+    B = PK.from_ints([2, (1 << 900) - 1, 11, -(1 << 70)])
+    st, sizes = _noalloc_raw(2, 2, 2, A, B, cap_delta=-1)
+    assert st == _lib.MPZMM_ERR_CAPACITY
+    assert sizes == [777] * 4
+    # and with the stated capacity the same call succeeds
+    st, sizes = _noalloc_raw(2, 2, 2, A, B)
+    assert st == _lib.MPZMM_OK
+    assert sizes != [777] * 4
