@@ -1,28 +1,35 @@
 // Tensor-core contraction (tcgen05.mma kind::i8, sm_100a), exact.
 //
 // Per frequency h and prime p: C = A B mod p with A (m x k), B (k x n)
-// residues in [0, p), p < 2^30.  Each residue is centred (v in (-p/2, p/2))
-// and split into balanced signed bytes v = d0 + 2^8 d1 + 2^16 d2 + 2^24 d3
-// (|d_s| <= 128, |d3| <= 33).  With
-//     A'[i, 4kk + s]       = a_s[i, kk]
-//     B'[8l + u, 4kk + s]  = b_{u-s}[kk, l]   (0 <= u - s <= 3, else 0)
-// the int8 GEMM D = A' B'^T (K' = 4k) gives D[i, 8l + u] =
-// sum_kk sum_s a_s b_{u-s}, the u-th digit convolution, so
-//     sum_kk a b = sum_{u=0..6} 2^(8u) D[i, 8l + u]
-// exactly; |D| <= 4k 2^14 fits the int32 accumulators for k < 2^15.  Column
-// 8l + 7 is padding (zero), which keeps each output's 8 columns aligned for
-// one tcgen05.ld.32x32b.x8.  The epilogue forms z = sum_u D_u (2^(8u) mod p)
-// in 64 bits (|z| < 2^56 for k <= 64), adds a bias that is a multiple of p,
-// and Montgomery-reduces, so the result carries the same 2^-32 factor as the
-// CUDA-core contraction.
+// residues below 2^32.  Each residue is its four unsigned bytes,
+// x = sum_s 2^(8s) x_s, so
+//     sum_kk A[i,kk] B[kk,l] = sum_{s,t} 2^(8(s+t)) D_st[i,l],
+//     D_st[i,l] = sum_kk a_s[i,kk] b_t[kk,l]      (0 <= D < k 2^16, exact in int32),
+// sixteen byte-plane products that one u8 x u8 GEMM computes at once:
+//   A' rows s m8 + i   (the four byte planes of A stacked along M, m8 = m
+//                       rounded up to 32, 64 or 128 rows a plane), bytes kk;
+//   B' rows 4 l + t    (the planes of B interleaved along N), bytes kk;
+//   D = A' B'^T        (M = 4 m8 in tiles of 128 TMEM lanes, N = 4 n).
+// Half the MACs of a Toeplitz-expanded split and no expansion of either
+// operand: the split is four byte permutes per four residues.  The epilogue
+// forms z = sum_{s,t} (2^(8(s+t)) mod p) D_st (< 2^57 for k <= 64) in 64 bits,
+// adding the partial sums of the lanes that hold the same row i, and
+// Montgomery-reduces it, so C carries the same 2^-32 factor as the CUDA-core
+// contraction.
 //
-// One CTA of 128 threads per (product, prime, block of frequencies): the
-// operands of one frequency are staged in shared memory in the canonical
-// K-major no-swizzle layout (8-row x 16-byte core matrices), one elected
-// thread issues the MMAs (M = 128 rows = TMEM lanes, N <= 256 per MMA,
-// K = 32 bytes per MMA), tcgen05.commit arrives on an mbarrier, and warp w
-// reads TMEM lanes 32w..32w+31.  Every wait is bounded (one second of wall
-// time): on time-out the CTA records an error, stops issuing work, frees its
+// One CTA of 256 threads per (product, prime, block of 16 frequencies),
+// processed F frequencies at a time: all warps stage A' and B' of the F
+// frequencies straight from global memory (F consecutive residues of a
+// polynomial per vector load) into canonical K-major no-swizzle tiles (8-row
+// x 16-byte core matrices; every st.shared of a warp hits 32 distinct
+// banks); one thread issues the MMAs of a unit (one frequency, up to 32 of
+// its output columns), tcgen05.commit arrives on the unit's mbarrier; with two
+// TMEM accumulators the next unit's MMAs run while all eight warps drain the
+// current one (warp w reads TMEM lanes 32 (w mod 4) .. + 31, the two
+// warpgroups take alternate 16-column chunks).  Results of the F
+// frequencies are gathered in shared memory and stored F residues per vector
+// store.  Every wait is bounded (one second of wall time): on time-out the
+// CTA records an error, waits (bounded) for MMAs it has issued, frees its
 // TMEM and returns.
 #pragma once
 
@@ -31,13 +38,66 @@
 namespace mpzmm {
 namespace tc {
 
-constexpr int kThreads = 128;
-constexpr int kMaxK = 64;        // k <= 64  -> K' <= 256 bytes
-constexpr int kMaxN = 64;        // n <= 64  -> 8n <= 512 TMEM columns
-constexpr int kMaxM = 128;       // one M = 128 tile
-constexpr int kTmemCols = 512;   // allocated per CTA (one CTA per SM by shared memory)
+constexpr int kThreads = 256;
+constexpr int kMaxK = 64;        // k <= 64: K' = k bytes padded to 32, z < 2^57
+constexpr int kMaxN = 64;        // n <= 64: at most two units of 32 outputs a frequency
+constexpr int kMaxM = 128;       // m <= 128: four planes in four 128-lane tiles
+constexpr int kFreqs = 16;       // frequencies per CTA
+constexpr int kUnitCols = 32;    // output columns l per unit
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // one second of wall time
+constexpr int kSmemLimit = 227 * 1024;  // shared memory of a block, static included
+constexpr int kStaticSmem = 1024;       // the kernel's barriers and TMEM slot (aligned)
+constexpr int kDynSmemLimit = kSmemLimit - kStaticSmem;
+
+// Shape of one product on the tensor cores (host and device).
+struct Shape {
+  int m8;      // rows per plane: 32, 64 or 128
+  int mt;      // 128-lane M tiles: 4 m8 / 128
+  int kp;      // K' bytes: k rounded up to 32
+  int npl;     // output columns per unit: min(n, 32)
+  int nunits;  // units per frequency: ceil(n / npl)
+  int ncol;    // MMA N of a unit: 4 npl rounded up to 16
+  int g;       // lanes holding one row i: 128 / m8
+  int a_bytes, b_bytes, red_bytes;
+};
+
+__host__ __device__ inline Shape shape_of(int m, int k, int n) {
+  Shape s;
+  s.m8 = m <= 32 ? 32 : (m <= 64 ? 64 : 128);
+  s.mt = 4 * s.m8 / 128;
+  s.kp = (k + 31) & ~31;
+  s.npl = n < kUnitCols ? n : kUnitCols;
+  s.nunits = (n + s.npl - 1) / s.npl;
+  s.ncol = (4 * s.npl + 15) & ~15;
+  s.g = 128 / s.m8;
+  s.a_bytes = 4 * s.m8 * s.kp;  // multiple of 4096
+  // B' rows: every unit's MMA reads ncol rows from row 4 npl u, and the
+  // staging writes rows 4 l + t for l up to n rounded up to 8
+  int brows = 4 * s.npl * (s.nunits - 1) + s.ncol;
+  if (brows < 4 * ((n + 7) & ~7)) brows = 4 * ((n + 7) & ~7);
+  s.b_bytes = ((brows * s.kp) + 1023) & ~1023;
+  s.red_bytes = s.g > 1 ? 128 * (s.npl + 1) * 8 : 0;
+  return s;
+}
+
+// TMEM columns of one accumulator (a unit) and whether two fit.
+__host__ __device__ inline int unit_cols(const Shape& s) { return s.mt * s.ncol; }
+__host__ __device__ inline bool double_buffered(const Shape& s) { return 2 * unit_cols(s) <= 512; }
+
+// Dynamic shared memory of a CTA for F frequencies at a time.
+__host__ __device__ inline int smem_bytes(const Shape& s, int m, int n, int F) {
+  const int out = ((m * n * F * 4) + 15) & ~15;
+  return F * (s.a_bytes + s.b_bytes) + s.red_bytes + out;
+}
+
+// TMEM columns to allocate: a power of two >= 32.
+__host__ __device__ inline int tmem_alloc_cols(const Shape& s) {
+  const int need = (double_buffered(s) ? 2 : 1) * unit_cols(s);
+  int c = 32;
+  while (c < need) c <<= 1;
+  return c;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -53,9 +113,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t kprime) {
   return d;                // base offset 0, legacy LBO mode, layout type 0
 }
 
-// kind::i8 instruction descriptor: D s32, A s8, B s8, both K-major, M = 128.
-__host__ __device__ constexpr uint32_t idesc_i8(uint32_t n) {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+// kind::i8 instruction descriptor: D s32, A u8, B u8, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_u8(uint32_t n) {
+  return (2u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
 // byte offset of (row, kbyte) in a K-major canonical tile with K' bytes/row
@@ -63,18 +123,15 @@ __device__ __forceinline__ uint32_t tile_off(uint32_t row, uint32_t kb, uint32_t
   return (row >> 3) * (8u * kprime) + (kb >> 4) * 128u + (row & 7u) * 16u + (kb & 15u);
 }
 
-// balanced signed bytes of the centred residue, packed byte s = d_s
-__device__ __forceinline__ uint32_t split_bytes(uint32_t x, uint32_t p) {
-  int32_t v = (int32_t)x - (x > (p >> 1) ? (int32_t)p : 0);
-  uint32_t packed = 0;
-#pragma unroll
-  for (int s = 0; s < 3; ++s) {
-    const int32_t d = (int32_t)(int8_t)(v & 0xff);
-    packed |= ((uint32_t)(uint8_t)d) << (8 * s);
-    v = (v - d) >> 8;
-  }
-  packed |= ((uint32_t)(uint8_t)v) << 24;  // |d3| <= 33
-  return packed;
+// byte planes of four residues: plane s = (x0_s, x1_s, x2_s, x3_s)
+__device__ __forceinline__ void byte_planes(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3,
+                                            uint32_t (&pl)[4]) {
+  const uint32_t lo01 = __byte_perm(x0, x1, 0x5140), hi01 = __byte_perm(x0, x1, 0x7362);
+  const uint32_t lo23 = __byte_perm(x2, x3, 0x5140), hi23 = __byte_perm(x2, x3, 0x7362);
+  pl[0] = __byte_perm(lo01, lo23, 0x5410);
+  pl[1] = __byte_perm(lo01, lo23, 0x7632);
+  pl[2] = __byte_perm(hi01, hi23, 0x5410);
+  pl[3] = __byte_perm(hi01, hi23, 0x7632);
 }
 
 __device__ __forceinline__ uint64_t global_ns() {

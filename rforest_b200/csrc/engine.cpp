@@ -224,6 +224,23 @@ int ensure_setup(int device) {
      "copy twiddles");
   CU(cudaMemcpy(g_ctx.d_twi, M.twi.data(), tw * sizeof(uint2), cudaMemcpyHostToDevice),
      "copy twiddles");
+  {
+    const size_t nt = (size_t)kMaxPrimes * kTwistEntries;
+    const size_t bytes = nt * (2 * sizeof(uint2) + 2 * sizeof(uint32_t));
+    CU(cudaMalloc(&g_ctx.d_twist, bytes), "cudaMalloc twist tables");
+    uint2* hf = static_cast<uint2*>(g_ctx.d_twist);
+    uint2* hi = hf + nt;
+    uint32_t* lf = reinterpret_cast<uint32_t*>(hi + nt);
+    uint32_t* li = lf + nt;
+    CU(cudaMemcpy(hf, M.twh_f.data(), nt * sizeof(uint2), cudaMemcpyHostToDevice), "copy twists");
+    CU(cudaMemcpy(hi, M.twh_i.data(), nt * sizeof(uint2), cudaMemcpyHostToDevice), "copy twists");
+    CU(cudaMemcpy(lf, M.twl_f.data(), nt * sizeof(uint32_t), cudaMemcpyHostToDevice),
+       "copy twists");
+    CU(cudaMemcpy(li, M.twl_i.data(), nt * sizeof(uint32_t), cudaMemcpyHostToDevice),
+       "copy twists");
+    g_ctx.twist_f = TwistTab{hf, lf};
+    g_ctx.twist_i = TwistTab{hi, li};
+  }
   CU(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking), "cudaStreamCreate");
   g_ctx.ws = new Workspace;
   if (const char* cm = std::getenv("MPZMM_CONTRACT")) {
@@ -242,6 +259,7 @@ void teardown() {
   cudaStreamSynchronize(g_ctx.stream);
   cudaFree(g_ctx.d_twf);
   cudaFree(g_ctx.d_twi);
+  cudaFree(g_ctx.d_twist);
   {
     std::lock_guard<std::mutex> wl(workspace_mutex());
     for (cudaStream_t s : g_ctx.pipe_st) {
@@ -634,6 +652,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     const bool use_tc = contract_tc_eligible(m, k, n) &&
                         (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)][tc_bucket_mn(m, n)] == 1));
     if (use_tc) {
+      if (m > tc_max_m_) tc_max_m_ = m;
       if (k > tc_max_k_) tc_max_k_ = k;
       if (n > tc_max_n_) tc_max_n_ = n;
     }
@@ -694,6 +713,12 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       const int D = fwd ? (g.max_r + 29) / 30 : 0;
       if (g.lgN < 3 || D > 7) {
         out.push_back(std::move(g));  // radix-2 path
+        continue;
+      }
+      if (g.lgN > kMaxLgNOneCta) {  // four-step transforms, a group per length
+        g.large = true;
+        g.D = D;
+        out.push_back(std::move(g));
         continue;
       }
       const bool team = ((int64_t)1 << g.lgN) <= (int64_t)fwd_team_points();
@@ -794,9 +819,9 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
   d_tc_items_ = reinterpret_cast<ContractItem*>(ws_->d_desc + off_tc_);
   d_idx_ = reinterpret_cast<uint32_t*>(ws_->d_desc + off_idx_);
   d_cta_ = reinterpret_cast<CtaItem*>(ws_->d_desc + off_cta_);
-  launches_ = (int64_t)fwd_groups_.size() + (items_.empty() ? 0 : 1) +
-              (tc_items_.empty() ? 0 : 1) +
-              (int64_t)inv_groups_.size() + (int64_t)rec_groups_.size();
+  int64_t sl[kStages];
+  stage_launches(sl);
+  launches_ = sl[0] + sl[1] + sl[2] + sl[3];
   built_ = true;
   return kOk;
 }
@@ -973,7 +998,11 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
     CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
   }
   for (const Group& g : fwd_groups_) {
-    if (g.batched)
+    if (g.large)
+      CU(launch_large_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.lgN, g.D,
+                          ws_->d_limbs, ws_->d_res, ctx.d_twf, ctx.twist_f, st),
+         "split+forward NTT launch (four-step)");
+    else if (g.batched)
       CU(launch_fwd_items(d_fwd_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.D, g.team,
                           g.max_lgN, ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
          "split+forward NTT launch");
@@ -986,12 +1015,16 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
   if (!tc_items_.empty())
-    CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, kTcFreqsPerCta,
+    CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, tc_max_m_,
                           tc_max_k_, tc_max_n_, ws_->d_status, st, take_test_stall_tc() ? 1 : 0),
        "tensor-core contraction launch");
   if (timed) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
   for (const Group& g : inv_groups_) {
-    if (g.batched)
+    if (g.large)
+      CU(launch_large_inv(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.lgN, ws_->d_res,
+                          ctx.d_twi, ctx.twist_i, st),
+         "inverse NTT launch (four-step)");
+    else if (g.batched)
       CU(launch_inv_items(d_inv_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.team,
                           g.max_lgN, ws_->d_res, ctx.d_twi, st),
          "inverse NTT launch");
@@ -1029,9 +1062,14 @@ int Plan::stage_times(float ms[kStages], int64_t* executes) {
 }
 
 void Plan::stage_launches(int64_t out[kStages]) const {
-  out[0] = (int64_t)fwd_groups_.size();
+  auto count = [](const std::vector<Group>& gs) {
+    int64_t n = 0;
+    for (const Group& g : gs) n += g.large ? kLargeLaunches : 1;
+    return n;
+  };
+  out[0] = count(fwd_groups_);
   out[1] = (items_.empty() ? 0 : 1) + (tc_items_.empty() ? 0 : 1);
-  out[2] = (int64_t)inv_groups_.size();
+  out[2] = count(inv_groups_);
   out[3] = (int64_t)rec_groups_.size();
 }
 

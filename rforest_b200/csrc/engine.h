@@ -115,6 +115,10 @@ struct Context {
   cudaStream_t stream = nullptr;
   uint2* d_twf = nullptr;
   uint2* d_twi = nullptr;
+  // four-step twist tables, one allocation (forward hi, inverse hi, then
+  // forward lo, inverse lo)
+  void* d_twist = nullptr;
+  TwistTab twist_f{nullptr, nullptr}, twist_i{nullptr, nullptr};
   int num_sms = 0;
   Workspace* ws = nullptr;  // shared by one-shot calls (guarded by ws_mu)
   // contraction engine: 0 automatic (tensor cores from kTcMinK terms on),
@@ -174,7 +178,7 @@ inline int tc_bucket_mn(int m, int n) {
   return b < 5 ? b : 4;
 }
 
-constexpr int kTcFreqsPerCta = 16;
+constexpr int kTcFreqsPerCta = 16;  // = contract_tc_freqs() (frequencies per tensor-core CTA)
 
 Context& context();
 std::mutex& workspace_mutex();
@@ -266,6 +270,7 @@ class Plan {
     // batched transform launch (several size classes, CTA work items)
     bool batched = false;
     bool team = false;
+    bool large = false;    // four-step transform (2^lgN above one CTA)
     int D = 0;
     int max_lgN = 0;
     std::vector<CtaItem> items;
@@ -283,7 +288,7 @@ class Plan {
   std::vector<ProdDesc> pd_;
   std::vector<ContractItem> items_;     // CUDA-core contraction work
   std::vector<ContractItem> tc_items_;  // tensor-core contraction work
-  int tc_max_k_ = 0, tc_max_n_ = 0;
+  int tc_max_m_ = 0, tc_max_k_ = 0, tc_max_n_ = 0;
   std::vector<Group> fwd_groups_, inv_groups_, rec_groups_;
   std::vector<uint32_t> idx_all_;
   std::vector<CtaItem> cta_items_;

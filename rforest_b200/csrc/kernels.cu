@@ -689,6 +689,311 @@ k_inv2(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Transforms longer than one CTA holds (2^16 .. 2^20 points): four steps on
+// the same tree.
+//
+// The forward tree's first lgR stages only combine points x = q C + lo with
+// the same lo (C = 2^kLargeLgC, R = N / C), and their twiddles T[m + i] do
+// not depend on N: for each of the C columns they are an ordinary R-point
+// forward transform.  Afterwards block b = [b C, (b + 1) C) (b = the row
+// position, already bit-reversed) holds a(X) mod (X^C - psi_b^C) with
+// psi_b = w_N^brev(b), and the remaining stages on the block equal the
+// twist y -> psi_b^y a_y followed by an ordinary C-point transform.  So:
+//   k_fwd_cols           split + column transforms + twist, on tiles of
+//                        R rows x W columns (R W = 2048 points: one group of
+//                        eight a thread, its digits kept in registers for all
+//                        P primes)
+//   k_ntt_blocks<true>   C-point transforms of the blocks (vector loads)
+// and the inverse the other way round:
+//   k_ntt_blocks<false>  inverse C-point transforms, untwist by psi_b^-y
+//   k_inv_cols           inverse column transforms, natural order out
+// The result is the same canonical evaluation at the same position as the
+// one-CTA transform, and the inverse again returns N times its input.
+// Twist factors W^E, W a primitive 2^20-th root with W^32 the 2^15 table's
+// root and E = brev(b) y 2^(20 - lgN), take one Shoup product of two table
+// entries (TwistTab) and one Montgomery product.
+// ---------------------------------------------------------------------------
+constexpr int kColPoints = 2048;  // points of a column tile (R x W)
+constexpr int kLgColPoints = 11;
+
+// x W^E mod p in [0, p) for x < 4p, E < 2^20 (tables of one prime)
+__device__ __forceinline__ uint32_t twist_mul(uint32_t x, uint32_t E,
+                                              const uint2* __restrict__ hi,
+                                              const uint32_t* __restrict__ lo, uint32_t p,
+                                              uint32_t pinv) {
+  const uint2 h = __ldg(hi + (E >> 10));
+  const uint32_t f = mul_shoup(__ldg(lo + (E & 1023u)), h.x, h.y, p);  // W^E 2^32 mod p
+  return redc((uint64_t)x * f, p, pinv);  // x f < 4 p^2 < p 2^32
+}
+
+// element (row q, column c) of a column tile with 2^lgW columns
+__device__ __forceinline__ int cti(int q, int c, int lgW) { return smi((q << lgW) + c); }
+
+// one pass of three stages (s0 .. s0 + 2) over every column of the tile
+template <bool FWD>
+__device__ __forceinline__ void col_pass3(uint32_t* s, int lgR, int lgW, int s0,
+                                          const uint2* __restrict__ tw, uint32_t p) {
+  const int lg_tmin = lgR - s0 - 3;
+  const int groups = (1 << (lgR - 3)) << lgW;
+  for (int gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+    const int c = gi & ((1 << lgW) - 1);
+    const int g = gi >> lgW;
+    const int lo = g & ((1 << lg_tmin) - 1);
+    const int hi = g >> lg_tmin;
+    const int base = (hi << (lg_tmin + 3)) + lo;
+    uint32_t a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = s[cti(base + (q << lg_tmin), c, lgW)];
+    if (FWD)
+      fwd_group<3>(a, s0, hi, tw, p);
+    else
+      inv_group<3>(a, s0, hi, tw, p);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[cti(base + (q << lg_tmin), c, lgW)] = a[q];
+  }
+}
+
+// the last forward column pass (LP stages from last_s0, groups of 2^LP
+// consecutive rows), twisted and stored to the polynomial `out`
+template <int LP>
+__device__ __forceinline__ void col_last_fwd(const uint32_t* s, uint32_t* __restrict__ out,
+                                             int lgR, int lgW, int lgN, int lo0, int last_s0,
+                                             const uint2* __restrict__ tw,
+                                             const uint2* __restrict__ th,
+                                             const uint32_t* __restrict__ tl, uint32_t p,
+                                             uint32_t pinv) {
+  const int groups = (1 << (lgR - LP)) << lgW;
+  for (int gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+    const int c = gi & ((1 << lgW) - 1);
+    const int hi = gi >> lgW;
+    uint32_t a[1 << LP];
+#pragma unroll
+    for (int q = 0; q < (1 << LP); ++q) a[q] = s[cti((hi << LP) + q, c, lgW)];
+    fwd_group<LP>(a, last_s0, hi, tw, p);
+    const uint32_t y = (uint32_t)(lo0 + c);
+#pragma unroll
+    for (int q = 0; q < (1 << LP); ++q) {
+      const uint32_t row = (uint32_t)((hi << LP) + q);
+      const uint32_t E = ((__brev(row) >> (32 - lgR)) * y) << (20 - lgN);
+      out[((uint64_t)row << kLargeLgC) + y] = twist_mul(a[q], E, th, tl, p, pinv);
+    }
+  }
+}
+
+// the last forward column pass inverted: groups of 2^LP consecutive rows
+// from the polynomial `in`, into the tile
+template <int LP>
+__device__ __forceinline__ void col_last_inv(uint32_t* s, const uint32_t* __restrict__ in,
+                                             int lgR, int lgW, int lo0, int last_s0,
+                                             const uint2* __restrict__ tw, uint32_t p) {
+  const int groups = (1 << (lgR - LP)) << lgW;
+  for (int gi = threadIdx.x; gi < groups; gi += blockDim.x) {
+    const int c = gi & ((1 << lgW) - 1);
+    const int hi = gi >> lgW;
+    uint32_t a[1 << LP];
+#pragma unroll
+    for (int q = 0; q < (1 << LP); ++q)
+      a[q] = in[((uint64_t)((hi << LP) + q) << kLargeLgC) + (uint32_t)(lo0 + c)];
+    inv_group<LP>(a, last_s0, hi, tw, p);
+#pragma unroll
+    for (int q = 0; q < (1 << LP); ++q) s[cti((hi << LP) + q, c, lgW)] = a[q];
+  }
+}
+
+// Split + column transforms + twist.  grid = entries x tiles (2 R tiles of
+// W = 2048 / R columns per entry); every entry of a launch has 2^lgN points.
+template <int D>
+__global__ void __launch_bounds__(kFwdThreads, 3)
+k_fwd_cols(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int tiles,
+           const uint64_t* __restrict__ limbs, uint32_t* __restrict__ res,
+           const uint2* __restrict__ twf, TwistTab tt) {
+  extern __shared__ uint32_t sm[];
+  const int e = blockIdx.x / tiles;
+  const int tile = blockIdx.x - e * tiles;
+  const FwdDesc d = descs[idx[e]];
+  const int lgN = d.lgN;
+  const int lgR = lgN - kLargeLgC;
+  const int lgW = kLgColPoints - lgR;
+  const int lo0 = tile << lgW;
+  const uint64_t N = (uint64_t)1 << lgN;
+  const uint32_t nl = (uint32_t)(d.size < 0 ? -d.size : d.size);
+  const uint32_t nw = nl < 0x40000000u ? 2u * nl : 0x80000000u;
+  const uint32_t* __restrict__ w32 = reinterpret_cast<const uint32_t*>(limbs + d.limb_off);
+  const bool neg = d.size < 0;
+  // first-pass group of this thread: rows k R/8 + g of column c
+  const int c = (int)threadIdx.x & ((1 << lgW) - 1);
+  const int g = (int)threadIdx.x >> lgW;
+  const int lgR8 = lgR - 3;
+  // no coefficient in the upper half of the transform: rows k >= 4 of every
+  // first-pass group are zero (uniform: one entry per CTA)
+  const bool hz = d.ncoef <= (uint32_t)(N >> 1);
+  uint32_t dg[8][D];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t x = ((uint32_t)((k << lgR8) + g) << kLargeLgC) + (uint32_t)(lo0 + c);
+    coeff_digits<D>(w32, nw, x * d.r, d.r, x < d.ncoef && !(hz && k >= 4), dg[k]);
+  }
+  const int last_s0 = ((lgR - 1) / 3) * 3;
+  for (int j = 0; j < (int)d.P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = twf + (size_t)j * kTwStride;
+    uint32_t a[8];
+    if (hz) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = digits_residue<D>(dg[k], j, neg);
+      fwd_stage0_upper_zero<3>(a, p);
+      fwd_group<3, 1>(a, 0, 0, tw, p);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) a[k] = digits_residue<D>(dg[k], j, neg);
+      fwd_group<3>(a, 0, 0, tw, p);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sm[cti((k << lgR8) + g, c, lgW)] = a[k];
+    __syncthreads();
+    for (int s0 = 3; s0 < last_s0; s0 += 3) {
+      col_pass3<true>(sm, lgR, lgW, s0, tw, p);
+      __syncthreads();
+    }
+    uint32_t* out = res + d.res_off + (uint64_t)j * N;
+    const uint2* th = tt.hi + (size_t)j * kTwistEntries;
+    const uint32_t* tl = tt.lo + (size_t)j * kTwistEntries;
+    const uint32_t pinv = c_primes[j].pinv;
+    switch (lgR - last_s0) {
+      case 1: col_last_fwd<1>(sm, out, lgR, lgW, lgN, lo0, last_s0, tw, th, tl, p, pinv); break;
+      case 2: col_last_fwd<2>(sm, out, lgR, lgW, lgN, lo0, last_s0, tw, th, tl, p, pinv); break;
+      default: col_last_fwd<3>(sm, out, lgR, lgW, lgN, lo0, last_s0, tw, th, tl, p, pinv); break;
+    }
+    __syncthreads();  // before the next prime overwrites the tile
+  }
+}
+
+// C-point transforms of the blocks.  grid = entries x R blocks.  Forward:
+// ordinary forward transform of each (twisted) block.  Inverse: ordinary
+// inverse transform, then the untwist psi_b^-y (tt holds the inverse twist
+// tables).  Descriptors: fdescs (forward) or idescs (inverse).
+template <bool FWD>
+__global__ void __launch_bounds__(kFwdThreads)
+k_ntt_blocks(const FwdDesc* __restrict__ fdescs, const InvDesc* __restrict__ idescs,
+             const uint32_t* __restrict__ idx, int blocks, uint32_t* __restrict__ res,
+             const uint2* __restrict__ tws, TwistTab tt) {
+  extern __shared__ uint32_t sm[];
+  const int e = blockIdx.x / blocks;
+  const int b = blockIdx.x - e * blocks;
+  uint64_t off;
+  int lgN, P;
+  if (FWD) {
+    const FwdDesc& d = fdescs[idx[e]];
+    off = d.res_off;
+    lgN = d.lgN;
+    P = d.P;
+  } else {
+    const InvDesc& d = idescs[idx[e]];
+    off = d.res_off;
+    lgN = d.lgN;
+    P = d.P;
+  }
+  constexpr int lgC = kLargeLgC;
+  constexpr int C = 1 << lgC;
+  constexpr int last_s0 = ((lgC - 1) / 3) * 3;
+  static_assert(lgC - last_s0 == 3, "the block length must end on a full pass");
+  const int lgR = lgN - lgC;
+  const uint64_t N = (uint64_t)1 << lgN;
+  const int tid = threadIdx.x;
+  const uint32_t bb = __brev((uint32_t)b) >> (32 - lgR);
+  for (int j = 0; j < P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = tws + (size_t)j * kTwStride;
+    uint32_t* io = res + off + (uint64_t)j * N + ((uint64_t)b << lgC);
+    if (FWD) {
+      for (int v = tid; v < C / 4; v += kFwdThreads) {
+        const uint4 u = reinterpret_cast<const uint4*>(io)[v];
+        sm[smi(4 * v)] = u.x;
+        sm[smi(4 * v + 1)] = u.y;
+        sm[smi(4 * v + 2)] = u.z;
+        sm[smi(4 * v + 3)] = u.w;
+      }
+      __syncthreads();
+      for (int s0 = 0; s0 < last_s0; s0 += 3) {
+        smem_pass<3, true>(sm, lgC, s0, 3, tid, kFwdThreads, tw, p);
+        __syncthreads();
+      }
+      fwd_last_pass<3>(sm, io, true, lgC, last_s0, tid, kFwdThreads, tw, p);
+      __syncthreads();
+    } else {
+      for (int g = tid; g < C / 8; g += kFwdThreads) {
+        uint32_t a[8];
+        load_points<3>(io + (g << 3), a);
+        inv_last_pass<3>(sm, a, g, last_s0, tw, p);
+      }
+      __syncthreads();
+      for (int s0 = last_s0 - 3; s0 >= 3; s0 -= 3) {
+        smem_pass<3, false>(sm, lgC, s0, 3, tid, kFwdThreads, tw, p);
+        __syncthreads();
+      }
+      const uint2* th = tt.hi + (size_t)j * kTwistEntries;
+      const uint32_t* tl = tt.lo + (size_t)j * kTwistEntries;
+      const uint32_t pinv = c_primes[j].pinv;
+      for (int g = tid; g < C / 8; g += kFwdThreads) {
+        uint32_t a[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[q] = sm[smi(q * (C / 8) + g)];
+        inv_group<3>(a, 0, 0, tw, p);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const uint32_t y = (uint32_t)(q * (C / 8) + g);
+          io[y] = twist_mul(a[q], (bb * y) << (20 - lgN), th, tl, p, pinv);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Inverse column transforms, natural coefficient order out (values in
+// [0, 2p), as the CRT expects).  grid = entries x tiles, as k_fwd_cols.
+__global__ void __launch_bounds__(kFwdThreads)
+k_inv_cols(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, int tiles,
+           uint32_t* __restrict__ res, const uint2* __restrict__ twi) {
+  extern __shared__ uint32_t sm[];
+  const int e = blockIdx.x / tiles;
+  const int tile = blockIdx.x - e * tiles;
+  const InvDesc d = descs[idx[e]];
+  const int lgN = d.lgN;
+  const int lgR = lgN - kLargeLgC;
+  const int lgW = kLgColPoints - lgR;
+  const int lo0 = tile << lgW;
+  const uint64_t N = (uint64_t)1 << lgN;
+  const int c = (int)threadIdx.x & ((1 << lgW) - 1);
+  const int g = (int)threadIdx.x >> lgW;
+  const int lgR8 = lgR - 3;
+  const int last_s0 = ((lgR - 1) / 3) * 3;
+  for (int j = 0; j < (int)d.P; ++j) {
+    const uint32_t p = c_primes[j].p;
+    const uint2* tw = twi + (size_t)j * kTwStride;
+    uint32_t* io = res + d.res_off + (uint64_t)j * N;
+    switch (lgR - last_s0) {
+      case 1: col_last_inv<1>(sm, io, lgR, lgW, lo0, last_s0, tw, p); break;
+      case 2: col_last_inv<2>(sm, io, lgR, lgW, lo0, last_s0, tw, p); break;
+      default: col_last_inv<3>(sm, io, lgR, lgW, lo0, last_s0, tw, p); break;
+    }
+    __syncthreads();
+    for (int s0 = last_s0 - 3; s0 >= 3; s0 -= 3) {
+      col_pass3<false>(sm, lgR, lgW, s0, tw, p);
+      __syncthreads();
+    }
+    uint32_t a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = sm[cti((k << lgR8) + g, c, lgW)];
+    inv_group<3>(a, 0, 0, tw, p);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      io[((uint64_t)((k << lgR8) + g) << kLargeLgC) + (uint32_t)(lo0 + c)] = a[k];
+    __syncthreads();  // before the next prime overwrites the tile
+  }
+}
+
 
 // ---------------------------------------------------------------------------
 // CRT + recompose, one warp per output entry (no block barriers).
@@ -955,13 +1260,79 @@ k_crt_mixed(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
 
 
 // ---------------------------------------------------------------------------
-// Tensor-core contraction (see contract_tc.cuh for the exact-split scheme).
+// Tensor-core contraction (byte-plane scheme: contract_tc.cuh).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :: "r"(d), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t barp) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(barp) : "memory");
+}
+
+// The MMAs of unit u (frequency u / nunits of the staged block, output
+// columns npl (u mod nunits) ..) into the accumulator at TMEM column dcol:
+// one M tile of 128 A' rows at a time, K' in steps of 32 bytes.
+__device__ __forceinline__ void tc_issue_unit(const tc::Shape& sh, uint32_t a_base,
+                                              uint32_t b_base, int u, uint32_t dcol) {
+  const int f = u / sh.nunits;
+  const int uu = u - f * sh.nunits;
+  const uint32_t kp = (uint32_t)sh.kp;
+  const uint32_t a0 = a_base + (uint32_t)(f * sh.a_bytes);
+  // B' row 4 npl uu (a multiple of 8: npl = 32 when there are several units)
+  const uint32_t b0 = b_base + (uint32_t)(f * sh.b_bytes) + (uint32_t)(4 * sh.npl * uu) * kp;
+  const uint32_t idesc = tc::idesc_u8((uint32_t)sh.ncol);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  for (int q = 0; q < sh.mt; ++q)
+    for (uint32_t ks = 0; ks < kp / 32; ++ks)
+      tc_mma(dcol + (uint32_t)(q * sh.ncol),
+             tc::smem_desc(a0 + 128u * (uint32_t)q * kp + 256u * ks, kp),
+             tc::smem_desc(b0 + 256u * ks, kp), idesc, ks > 0 ? 1u : 0u);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// F consecutive residues (frequencies hs .. hs + F - 1) of one polynomial;
+// only nf of them exist when the transform is shorter than the block
+template <int F>
+__device__ __forceinline__ void load_freqs(const uint32_t* src, bool ok, int nf,
+                                           uint32_t (&x)[F]) {
+  if (ok && nf == F && F >= 4) {
+#pragma unroll
+    for (int c = 0; c < F / 4; ++c) {
+      const uint4 u = __ldg(reinterpret_cast<const uint4*>(src) + c);
+      x[4 * c] = u.x;
+      x[4 * c + 1] = u.y;
+      x[4 * c + 2] = u.z;
+      x[4 * c + 3] = u.w;
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < F; ++f) x[f] = (ok && f < nf) ? __ldg(src + f) : 0u;
+  }
+}
+
+template <int F>
 __global__ void __launch_bounds__(tc::kThreads, 1)
 k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
-              uint32_t* __restrict__ res, int fb, int* __restrict__ status, int stall) {
+              uint32_t* __restrict__ res, int tmem_cols, int* __restrict__ status, int stall) {
   extern __shared__ __align__(1024) uint8_t tsm[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -972,127 +1343,214 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   const int N = 1 << d.lgN;
   const int j = it.prime;
   const uint32_t p = c_primes[j].p;
+  const uint32_t pinv = c_primes[j].pinv;
+  const uint32_t mu = c_primes[j].mu;
   const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
-  const uint32_t kprime = (uint32_t)((4 * k + 31) & ~31);
-  const uint32_t ncols = (uint32_t)((8 * n + 15) & ~15);  // B' rows = D columns
+  const tc::Shape sh = tc::shape_of(m, k, n);
+  const bool dbl = tc::double_buffered(sh);
+  const uint32_t ucols = (uint32_t)tc::unit_cols(sh);
+  const int plane_bytes = sh.m8 * sh.kp;
   uint8_t* As = tsm;
-  uint8_t* Bs = tsm + 128u * kprime;
-  const uint32_t tile_bytes = (128u + ncols) * kprime;
+  uint8_t* Bs = As + F * sh.a_bytes;
+  uint64_t* red = reinterpret_cast<uint64_t*>(Bs + F * sh.b_bytes);
+  uint32_t* outs = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(red) + sh.red_bytes);
+  const uint32_t a_base = tc::smem_u32(As), b_base = tc::smem_u32(Bs);
+  const uint32_t barp[2] = {tc::smem_u32(&bars[0]), tc::smem_u32(&bars[1])};
 
-  // zero both tiles once: padding rows/columns stay zero for every frequency
-  for (uint32_t o = 16u * tid; o < tile_bytes; o += 16u * tc::kThreads)
-    *reinterpret_cast<uint4*>(tsm + o) = make_uint4(0, 0, 0, 0);
   if (warp == 0) {
     const uint32_t slot = tc::smem_u32(&tmem_slot);
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 :: "r"(slot), "r"((uint32_t)tc::kTmemCols) : "memory");
+                 :: "r"(slot), "r"((uint32_t)tmem_cols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(tc::smem_u32(&bar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(barp[0]) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(barp[1]) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
-  const uint32_t barp = tc::smem_u32(&bar);
-  uint32_t phase = 0;
-  const uint64_t bias = c_primes[j].bias;
-  const uint32_t pinv = c_primes[j].pinv;
-  const uint32_t mu = c_primes[j].mu;
+  // commits issued and not yet waited for, and the parity to wait for, per
+  // accumulator (the same on every thread)
+  uint32_t phase[2] = {0u, 0u};
+  int pending[2] = {0, 0};
+  bool failed = false;
+  const int issue = stall ? 0 : 1;  // stall (failure-path tests only): no MMA, no commit
 
-  for (int f = 0; f < fb; ++f) {
-    const uint32_t h = it.h0 + (uint32_t)f;
-    if (h >= (uint32_t)N) break;  // uniform over the CTA
-    const uint64_t base = (uint64_t)j * (uint64_t)N + h;
-    // stage A' (row i, bytes 4kk..4kk+3) and B' (rows 8l+u, same bytes)
-    for (int idx = tid; idx < m * k; idx += tc::kThreads) {
-      const int i = idx / k, kk = idx - (idx / k) * k;
-      const uint32_t x = __ldg(res + d.a_res + (uint64_t)(i * k + kk) * stride + base);
-      *reinterpret_cast<uint32_t*>(As + tc::tile_off((uint32_t)i, 4u * kk, kprime)) =
-          tc::split_bytes(x, p);
-    }
-    for (int idx = tid; idx < k * n; idx += tc::kThreads) {
-      const int kk = idx / n, l = idx - (idx / n) * n;
-      const uint32_t x = __ldg(res + d.b_res + (uint64_t)(kk * n + l) * stride + base);
-      const uint32_t rev = __byte_perm(tc::split_bytes(x, p), 0u, 0x0123u);  // d3 d2 d1 d0
-      const uint64_t T = (uint64_t)rev << 32;
+  for (int fb0 = 0; fb0 < tc::kFreqs; fb0 += F) {
+    const uint32_t hs = it.h0 + (uint32_t)fb0;
+    if (hs >= (uint32_t)N) break;  // uniform over the CTA
+    const int nf = (int)((uint32_t)N - hs < (uint32_t)F ? (uint32_t)N - hs : (uint32_t)F);
+    const uint64_t base = (uint64_t)j * (uint64_t)N + hs;
+
+    // ---- stage A' and B' of the nf frequencies: a warp task is 8 rows
+    // (i of A, l of B) by 16 terms; a thread gathers four terms' residues
+    // of one row for every frequency and writes their byte planes
+    const int kbn = sh.kp / 16;
+    const int a_tasks = ((m + 7) / 8) * kbn;
+    const int tasks = a_tasks + ((n + 7) / 8) * kbn;
+    for (int task = warp; task < tasks; task += tc::kThreads / 32) {
+      const bool isA = task < a_tasks;
+      const int tt = isA ? task : task - a_tasks;
+      const int rb = tt / kbn;
+      const int kb = tt - rb * kbn;
+      const int kk0 = 16 * kb + 4 * (lane & 3);
+      // A: lane -> (row i mod 8, term quad); B: lane -> (l mod 8, term quad)
+      const int r = 8 * rb + (isA ? ((lane >> 2) & 7) : (lane >> 2));
+      uint32_t x[4][F];
 #pragma unroll
-      for (int u = 0; u < 7; ++u)
-        *reinterpret_cast<uint32_t*>(Bs + tc::tile_off((uint32_t)(8 * l + u), 4u * kk, kprime)) =
-            (uint32_t)(T >> (8 * (7 - u)));
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    // stall (failure-path tests only): no MMA and no commit are issued, so
-    // nothing ever arrives on the barrier and the bounded wait below runs out
-    // with no tensor operation outstanding
-    if (tid == 0 && !stall) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (uint32_t t0 = 0; t0 < ncols; t0 += 256) {
-        const uint32_t nt = (ncols - t0) < 256u ? (ncols - t0) : 256u;
-        const uint32_t idesc = tc::idesc_i8(nt);
-        for (uint32_t ks = 0; ks < kprime / 32; ++ks) {
-          const uint64_t ad = tc::smem_desc(tc::smem_u32(As) + 256u * ks, kprime);
-          const uint64_t bd = tc::smem_desc(tc::smem_u32(Bs) + t0 * kprime + 256u * ks, kprime);
-          const uint32_t acc = ks > 0 ? 1u : 0u;
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-              :: "r"(tmem + t0), "l"(ad), "l"(bd), "r"(idesc), "r"(acc),
-                 "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-              : "memory");
-        }
+      for (int c = 0; c < 4; ++c) {
+        const int kk = kk0 + c;
+        const bool ok = kk < k && r < (isA ? m : n);
+        const uint64_t poly = ok ? (isA ? (uint64_t)(r * k + kk) : (uint64_t)(kk * n + r)) : 0;
+        const uint32_t* src = res + (isA ? d.a_res : d.b_res) + poly * stride + base;
+        load_freqs<F>(src, ok, nf, x[c]);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(barp) : "memory");
-    }
-    const bool ok = tc::mbar_wait(barp, phase);
-    phase ^= 1u;
-    if (__syncthreads_or(!ok)) {  // every thread takes the same branch
-      if (tid == 0) atomicExch(status, 1);
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // epilogue: warp w owns TMEM lanes 32w..32w+31 = rows i
-    const int i = 32 * warp + lane;
-    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
-    for (int l0 = 0; l0 < n; l0 += 4) {
-      uint32_t v[32];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-            "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-            "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
-            "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-            "=r"(v[30]), "=r"(v[31])
-          : "r"(lane_addr + 8u * (uint32_t)l0));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (i < m) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int l = l0 + q;
-          if (l < n) {
-            int64_t z = 0;
+      for (int f = 0; f < F; ++f) {
+        if (f >= nf) break;
+        uint32_t pl[4];
+        tc::byte_planes(x[0][f], x[1][f], x[2][f], x[3][f], pl);
+        if (isA) {
+          // plane s of row i: rows s m8 + i; lanes cover (i mod 8, quad): no conflicts
+          uint8_t* t = As + f * sh.a_bytes + tc::tile_off((uint32_t)r, (uint32_t)kk0,
+                                                          (uint32_t)sh.kp);
 #pragma unroll
-            for (int u = 0; u < 7; ++u) z += (int64_t)(int32_t)v[8 * q + u] * c_primes[j].w8[u];
-            const uint32_t out = redc64((uint64_t)(z + (int64_t)bias), p, pinv, mu);
-            res[d.c_res + (uint64_t)(i * n + l) * stride + base] = out;
+          for (int s = 0; s < 4; ++s) *reinterpret_cast<uint32_t*>(t + s * plane_bytes) = pl[s];
+        } else {
+          // plane t of column l: row 4 l + t; the store order rotates with
+          // bits 3-4 of the lane so every store covers all 32 banks
+          uint8_t* t = Bs + f * sh.b_bytes;
+          const int g = (lane >> 3) & 3;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int tp = (q + g) & 3;
+            const uint32_t v = tp == 0 ? pl[0] : (tp == 1 ? pl[1] : (tp == 2 ? pl[2] : pl[3]));
+            *reinterpret_cast<uint32_t*>(
+                t + tc::tile_off((uint32_t)(4 * r + tp), (uint32_t)kk0, (uint32_t)sh.kp)) = v;
           }
         }
       }
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
+
+    // ---- units: MMAs, then the epilogue of each ----
+    const int U = nf * sh.nunits;
+    if (tid == 0 && issue) {
+      tc_issue_unit(sh, a_base, b_base, 0, tmem);
+      tc_commit(barp[0]);
+    }
+    pending[0] += issue;
+    for (int u = 0; u < U; ++u) {
+      const int buf = dbl ? (u & 1) : 0;
+      if (dbl && u + 1 < U) {  // the next unit's MMAs overlap this epilogue
+        const int nb = (u + 1) & 1;
+        if (tid == 0 && issue) {
+          tc_issue_unit(sh, a_base, b_base, u + 1, tmem + (uint32_t)nb * ucols);
+          tc_commit(barp[nb]);
+        }
+        pending[nb] += issue;
+      }
+      const bool ok = tc::mbar_wait(barp[buf], phase[buf]);
+      if (ok) {
+        phase[buf] ^= 1u;
+        pending[buf] -= 1;
+      }
+      if (__syncthreads_or(!ok)) {  // every thread takes the same branch
+        failed = true;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int f = u / sh.nunits;
+      const int l0 = (u - f * sh.nunits) * sh.npl;
+      const int nl = (n - l0) < sh.npl ? (n - l0) : sh.npl;
+      const int nch = (nl + 3) / 4;
+      const int qd = warp & 3;
+      const int lam = 32 * qd + lane;  // this thread's TMEM lane
+      const int i = lam % sh.m8;       // its row (the same in every M tile)
+      const uint32_t laddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)buf * ucols;
+      for (int ch = warp >> 2; ch < nch; ch += 2) {  // warpgroups take alternate chunks
+        uint64_t part[4] = {0, 0, 0, 0};
+        for (int q = 0; q < sh.mt; ++q) {
+          uint32_t v[16];
+          tmem_ld16(laddr + (uint32_t)(q * sh.ncol + 16 * ch), v);
+          const int s = (128 * q + lam) / sh.m8;  // byte plane of this lane: warp-uniform
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const uint64_t w = c_primes[j].w8[s + t];
+#pragma unroll
+            for (int u2 = 0; u2 < 4; ++u2) part[u2] += (uint64_t)v[4 * u2 + t] * w;
+          }
+        }
+        if (sh.g == 1) {  // all four planes of row i are in this lane
+          if (i < m) {
+#pragma unroll
+            for (int u2 = 0; u2 < 4; ++u2) {
+              const int l = 4 * ch + u2;
+              if (l < nl) outs[(i * n + l0 + l) * F + f] = redc64(part[u2], p, pinv, mu);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int u2 = 0; u2 < 4; ++u2) {
+            const int l = 4 * ch + u2;
+            if (l < nl) red[lam * (sh.npl + 1) + l] = part[u2];
+          }
+        }
+      }
+      if (sh.g > 1) {  // add the partial sums of the g lanes that hold row i
+        __syncthreads();
+        for (int xo = tid; xo < m * nl; xo += tc::kThreads) {
+          const int ii = xo / nl, l = xo - ii * nl;
+          uint64_t z = 0;
+          for (int g2 = 0; g2 < sh.g; ++g2) z += red[(g2 * sh.m8 + ii) * (sh.npl + 1) + l];
+          outs[(ii * n + l0 + l) * F + f] = redc64(z, p, pinv, mu);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      if (!dbl && u + 1 < U) {
+        if (tid == 0 && issue) {
+          tc_issue_unit(sh, a_base, b_base, u + 1, tmem);
+          tc_commit(barp[0]);
+        }
+        pending[0] += issue;
+      }
+    }
+    if (failed) break;
+    // ---- the nf frequencies of every output, F residues a vector store ----
+    for (int e = tid; e < m * n; e += tc::kThreads) {
+      uint32_t* dst = res + d.c_res + (uint64_t)e * stride + base;
+      const uint32_t* sv = outs + e * F;
+      if (nf == F && F >= 4) {
+#pragma unroll
+        for (int c = 0; c < F / 4; ++c)
+          reinterpret_cast<uint4*>(dst)[c] =
+              make_uint4(sv[4 * c], sv[4 * c + 1], sv[4 * c + 2], sv[4 * c + 3]);
+      } else {
+        for (int f = 0; f < nf; ++f) dst[f] = sv[f];
+      }
+    }
+    __syncthreads();  // before the next block overwrites tiles and results
   }
+  if (failed) {
+    if (tid == 0) atomicExch(status, 1);
+    // MMAs already issued must finish before their TMEM is freed
+    for (int b = 0; b < 2; ++b)
+      while (pending[b] > 0) {
+        if (!tc::mbar_wait(barp[b], phase[b])) break;
+        phase[b] ^= 1u;
+        pending[b] -= 1;
+      }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-                 :: "r"(tmem), "r"((uint32_t)tc::kTmemCols) : "memory");
+                 :: "r"(tmem), "r"((uint32_t)tmem_cols) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -1324,6 +1782,62 @@ cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const Ct
   return cudaGetLastError();
 }
 
+// shared memory of the four-step kernels
+static size_t col_tile_bytes() { return sizeof(uint32_t) * (size_t)(kColPoints + (kColPoints >> 5)); }
+static size_t block_bytes() {
+  return sizeof(uint32_t) * (size_t)((1 << kLargeLgC) + ((1 << kLargeLgC) >> 5));
+}
+
+template <int D>
+static void launch_fwd_cols_d(int grid, cudaStream_t st, const FwdDesc* descs, const uint32_t* idx,
+                              int tiles, const uint64_t* limbs, uint32_t* res, const uint2* twf,
+                              const TwistTab& tt) {
+  k_fwd_cols<D><<<grid, kFwdThreads, col_tile_bytes(), st>>>(descs, idx, tiles, limbs, res, twf,
+                                                             tt);
+}
+
+int large_tiles(int lgN) { return 1 << (lgN - kLargeLgC + 1); }
+
+cudaError_t launch_large_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int lgN, int D,
+                             const uint64_t* limbs, uint32_t* res, const uint2* twf,
+                             const TwistTab& tt, cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  if (lgN <= kMaxLgNOneCta || lgN > kMaxLgN) return cudaErrorInvalidValue;
+  const int tiles = large_tiles(lgN);
+  const int blocks = 1 << (lgN - kLargeLgC);
+  const int grid = count * tiles;
+  switch (D) {
+    case 1: launch_fwd_cols_d<1>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 2: launch_fwd_cols_d<2>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 3: launch_fwd_cols_d<3>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 4: launch_fwd_cols_d<4>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 5: launch_fwd_cols_d<5>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 6: launch_fwd_cols_d<6>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    case 7: launch_fwd_cols_d<7>(grid, st, descs, idx, tiles, limbs, res, twf, tt); break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_ntt_blocks<true><<<count * blocks, kFwdThreads, block_bytes(), st>>>(descs, nullptr, idx,
+                                                                         blocks, res, twf, tt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_large_inv(const InvDesc* descs, const uint32_t* idx, int count, int lgN,
+                             uint32_t* res, const uint2* twi, const TwistTab& tt,
+                             cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  if (lgN <= kMaxLgNOneCta || lgN > kMaxLgN) return cudaErrorInvalidValue;
+  const int tiles = large_tiles(lgN);
+  const int blocks = 1 << (lgN - kLargeLgC);
+  k_ntt_blocks<false><<<count * blocks, kFwdThreads, block_bytes(), st>>>(nullptr, descs, idx,
+                                                                          blocks, res, twi, tt);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_inv_cols<<<count * tiles, kFwdThreads, col_tile_bytes(), st>>>(descs, idx, tiles, res, twi);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_split_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int P,
                              int lgN, const uint64_t* limbs, uint32_t* res,
                              const uint2* twf, cudaStream_t st) {
@@ -1356,18 +1870,55 @@ bool contract_tc_eligible(int m, int k, int n) {
   return m >= 1 && m <= tc::kMaxM && k >= 1 && k <= tc::kMaxK && n >= 1 && n <= tc::kMaxN;
 }
 
+// Frequencies staged at once (F), dynamic shared memory and TMEM columns of a
+// tensor-core launch whose products have at most max_m rows, max_k terms and
+// max_n columns: per-product layouts are all within these bounds.
+static bool tc_launch_config(int max_m, int max_k, int max_n, int* F, int* smem, int* tcols) {
+  const tc::Shape sh = tc::shape_of(max_m, max_k, max_n);
+  const int red = 128 * (sh.npl + 1) * 8;  // any product with fewer rows may need it
+  const int budget = tc::kDynSmemLimit;
+  for (int f = 16; f >= 1; f >>= 1) {
+    const int out = ((max_m * max_n * f * 4) + 15) & ~15;
+    const int bytes = f * (sh.a_bytes + sh.b_bytes) + red + out;
+    if (bytes <= budget) {
+      *F = f;
+      *smem = bytes;
+      const int uc = tc::unit_cols(sh);
+      int need = 2 * uc <= 512 ? 2 * uc : 512;
+      int c = 32;
+      while (c < need) c <<= 1;
+      *tcols = c;
+      return true;
+    }
+  }
+  return false;
+}
+
+template <int F>
+static void launch_tc_f(int count, int smem, cudaStream_t st, const ProdDesc* prods,
+                        const ContractItem* items, uint32_t* res, int tcols, int* status,
+                        int stall) {
+  k_contract_tc<F><<<count, tc::kThreads, smem, st>>>(prods, items, res, tcols, status, stall);
+}
+
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
-                               uint32_t* res, int fb, int max_k, int max_n, int* status,
+                               uint32_t* res, int max_m, int max_k, int max_n, int* status,
                                cudaStream_t st, int stall) {
   if (count == 0) return cudaSuccess;
-  const size_t kprime = (size_t)((4 * max_k + 31) & ~31);
-  const size_t ncols = (size_t)((8 * max_n + 15) & ~15);
-  size_t smem = (128 + ncols) * kprime;
-  // at least 120 KB so that one CTA (512 TMEM columns) runs per SM
-  if (smem < 120 * 1024) smem = 120 * 1024;
-  k_contract_tc<<<count, tc::kThreads, smem, st>>>(prods, items, res, fb, status, stall);
+  if (!contract_tc_eligible(max_m, max_k, max_n)) return cudaErrorInvalidValue;
+  int F = 0, smem = 0, tcols = 0;
+  if (!tc_launch_config(max_m, max_k, max_n, &F, &smem, &tcols)) return cudaErrorInvalidValue;
+  switch (F) {
+    case 16: launch_tc_f<16>(count, smem, st, prods, items, res, tcols, status, stall); break;
+    case 8: launch_tc_f<8>(count, smem, st, prods, items, res, tcols, status, stall); break;
+    case 4: launch_tc_f<4>(count, smem, st, prods, items, res, tcols, status, stall); break;
+    case 2: launch_tc_f<2>(count, smem, st, prods, items, res, tcols, status, stall); break;
+    default: launch_tc_f<1>(count, smem, st, prods, items, res, tcols, status, stall); break;
+  }
   return cudaGetLastError();
 }
+
+int contract_tc_freqs() { return tc::kFreqs; }
 
 // coefficients a CRT tile can touch for coefficient width rmin
 static int crt_cmax(int P, int rmin) {
@@ -1449,7 +2000,8 @@ cudaError_t launch_crt_recompose(const InvDesc* descs, const uint32_t* idx, int 
 // issue nothing but stream work).
 template <int D>
 static cudaError_t set_fwd_attrs() {
-  const int big = (int)(sizeof(uint32_t) * ((1 << kMaxLgN) + ((1 << kMaxLgN) >> 5)));
+  const int big =
+      (int)(sizeof(uint32_t) * ((1 << kMaxLgNOneCta) + ((1 << kMaxLgNOneCta) >> 5)));
   cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   if (e != cudaSuccess) return e;
@@ -1464,12 +2016,13 @@ static cudaError_t set_crt_attr() {
 
 cudaError_t init_kernel_attributes() {
   cudaError_t e;
-  const int big = (int)(sizeof(uint32_t) * ((1 << kMaxLgN) + ((1 << kMaxLgN) >> 5)));
+  const int big =
+      (int)(sizeof(uint32_t) * ((1 << kMaxLgNOneCta) + ((1 << kMaxLgNOneCta) >> 5)));
   if ((e = cudaFuncSetAttribute(k_split_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(uint32_t) << kMaxLgN))) != cudaSuccess)
+                                (int)(sizeof(uint32_t) << kMaxLgNOneCta))) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(k_inv_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(uint32_t) << kMaxLgN))) != cudaSuccess)
+                                (int)(sizeof(uint32_t) << kMaxLgNOneCta))) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(k_inv2<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) !=
       cudaSuccess)
@@ -1498,8 +2051,12 @@ cudaError_t init_kernel_attributes() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
           cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(k_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)((128 + 8 * tc::kMaxN) * 4 * tc::kMaxK));
+  for (auto fn : {k_contract_tc<16>, k_contract_tc<8>, k_contract_tc<4>, k_contract_tc<2>,
+                  k_contract_tc<1>})
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tc::kDynSmemLimit)) != cudaSuccess)
+      return e;
+  return cudaSuccess;
 }
 
 }  // namespace mpzmm

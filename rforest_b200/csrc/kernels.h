@@ -31,6 +31,19 @@ cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const Ct
                              int nitems, bool team, int max_lgN, uint32_t* res,
                              const uint2* twi, cudaStream_t st);
 
+// Transforms of 2^16 .. 2^20 points (four-step: column transforms, twist,
+// block transforms), `count` entries of one length 2^lgN in one group (idx
+// lists their descriptors).  Forward: split of D-digit coefficients + the
+// transform; inverse: the transform back to natural order, ready for the
+// CRT.  Two launches each.  tt: the twist tables of the direction.
+cudaError_t launch_large_fwd(const FwdDesc* descs, const uint32_t* idx, int count, int lgN, int D,
+                             const uint64_t* limbs, uint32_t* res, const uint2* twf,
+                             const TwistTab& tt, cudaStream_t st);
+cudaError_t launch_large_inv(const InvDesc* descs, const uint32_t* idx, int count, int lgN,
+                             uint32_t* res, const uint2* twi, const TwistTab& tt,
+                             cudaStream_t st);
+constexpr int kLargeLaunches = 2;  // kernel launches per direction of a four-step group
+
 // CUDA-core contraction over `count` work items.
 cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, int count,
                             uint32_t* res, cudaStream_t st);
@@ -48,12 +61,14 @@ cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_
                               cudaStream_t st);
 
 // Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
-// k <= 64, n <= 64; each work item covers `fb` consecutive frequencies.
-// *status is set to 1 if a bounded wait gave up.  stall != 0 (failure-path
-// tests only) issues no tensor work, so every CTA's wait runs out.
+// k <= 64, n <= 64 (max_m, max_k, max_n: the launch's largest); each work
+// item covers contract_tc_freqs() consecutive frequencies.  *status is set
+// to 1 if a bounded wait gave up.  stall != 0 (failure-path tests only)
+// issues no tensor work, so every CTA's wait runs out.
 bool contract_tc_eligible(int m, int k, int n);
+int contract_tc_freqs();
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
-                               uint32_t* res, int fb, int max_k, int max_n, int* status,
+                               uint32_t* res, int max_m, int max_k, int max_n, int* status,
                                cudaStream_t st, int stall = 0);
 
 // CRT + recompose + sign for `count` output entries with P primes; rmin is

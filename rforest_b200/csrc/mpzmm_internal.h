@@ -8,6 +8,8 @@
 // exact integer either way.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
 
@@ -15,8 +17,15 @@ namespace mpzmm {
 
 constexpr int kMaxPrimes = 16;      // primes available to a product
 constexpr int kPrimeLgRoot = 20;    // every prime is 1 mod 2^20
-constexpr int kMaxLgN = 15;         // largest transform handled in one CTA
-constexpr int kTwiddleLg = kMaxLgN; // twiddle tables cover N <= 2^kTwiddleLg
+constexpr int kMaxLgN = 20;         // largest transform (2^20 points: p = 1 mod 2^20)
+constexpr int kMaxLgNOneCta = 15;   // largest transform done in one CTA
+constexpr int kTwiddleLg = 15;      // twiddle tables cover N <= 2^15; every pass of
+                                    // a longer (four-step) transform is shorter
+constexpr int kLargeLgC = 12;       // block length of a four-step transform's second pass
+constexpr int kTwistEntries = 1024; // entries of each twist table per prime
+static_assert(kMaxLgN <= kPrimeLgRoot, "transform longer than the primes' 2-power roots");
+static_assert(kMaxLgN - kLargeLgC <= kTwiddleLg, "four-step columns beyond the table");
+static_assert(2 * 10 == kPrimeLgRoot, "twist exponents are split 10 + 10 bits");
 constexpr int kMaxCoeffBits = 192;  // largest split coefficient (r)
 constexpr int kMaxCrtWords = kMaxPrimes + 1;  // 32-bit words of a CRT value
 
@@ -53,6 +62,14 @@ struct CrtConst {
   // N = 2^lgN: removes the contraction's 2^-32 and the inverse transform's N
   uint32_t cm[kMaxPrimes + 1][kMaxLgN + 1][kMaxPrimes];
   uint32_t fq[kMaxPrimes];                           // floor(2^58 / p_j)
+};
+
+// Twist tables of the four-step transforms, one direction: per prime,
+// hi[u] = {W^(1024 u), its Shoup companion} and lo[v] = W^v 2^32 mod p for
+// u, v < 1024, W a primitive 2^20-th root (inverse direction: W^-1).
+struct TwistTab {
+  const uint2* hi;
+  const uint32_t* lo;
 };
 
 // One polynomial (one matrix entry) of the forward transform.

@@ -129,6 +129,10 @@ void build(Moduli& M) {
   const int TS = 1 << kTwiddleLg;
   M.twf.assign((size_t)kMaxPrimes * TS, make_uint2(0, 0));
   M.twi.assign((size_t)kMaxPrimes * TS, make_uint2(0, 0));
+  M.twh_f.assign((size_t)kMaxPrimes * kTwistEntries, make_uint2(0, 0));
+  M.twh_i.assign((size_t)kMaxPrimes * kTwistEntries, make_uint2(0, 0));
+  M.twl_f.assign((size_t)kMaxPrimes * kTwistEntries, 0);
+  M.twl_i.assign((size_t)kMaxPrimes * kTwistEntries, 0);
   for (int j = 0; j < kMaxPrimes; ++j) {
     const uint32_t p = M.p[j];
     PrimeConst& pc = M.pc[j];
@@ -145,6 +149,25 @@ void build(Moduli& M) {
     pc.bias = ((((uint64_t)1 << 56) + p - 1) / p) * p;
     const uint32_t g = primitive_root(p);
     const uint64_t wmax = powmod(g, (p - 1) >> kTwiddleLg, p);  // order 2^kTwiddleLg
+    {
+      // twist tables: W = g^((p-1)/2^20), so W^(2^(20-kTwiddleLg)) = wmax
+      const uint64_t W = powmod(g, (p - 1) >> kPrimeLgRoot, p);
+      const uint64_t Wi = powmod(W, p - 2, p);
+      const uint64_t r32 = (((uint64_t)1) << 32) % p;
+      const size_t o = (size_t)j * kTwistEntries;
+      uint64_t hf = 1, hi = 1, lf = 1, li = 1;
+      const uint64_t Wk = powmod(W, kTwistEntries, p), Wik = powmod(Wi, kTwistEntries, p);
+      for (int u = 0; u < kTwistEntries; ++u) {
+        M.twh_f[o + u] = make_uint2((uint32_t)hf, shoup((uint32_t)hf, p));
+        M.twh_i[o + u] = make_uint2((uint32_t)hi, shoup((uint32_t)hi, p));
+        M.twl_f[o + u] = (uint32_t)(lf * r32 % p);
+        M.twl_i[o + u] = (uint32_t)(li * r32 % p);
+        hf = hf * Wk % p;
+        hi = hi * Wik % p;
+        lf = lf * W % p;
+        li = li * Wi % p;
+      }
+    }
     for (int lgm = 0; lgm < kTwiddleLg; ++lgm) {
       const uint32_t m = 1u << lgm;
       // w_{2m} = wmax^(TS / (2m))

@@ -17,6 +17,10 @@ struct Moduli {
   int mbits[kMaxPrimes + 1];   // floor(log2(p_0 ... p_{P-1}))
   std::vector<uint2> twf;      // [kMaxPrimes][1 << kTwiddleLg] forward {w, wq}
   std::vector<uint2> twi;      // inverse
+  // twist tables of the four-step transforms ([kMaxPrimes][kTwistEntries]
+  // each; see TwistTab): forward (W) and inverse (W^-1)
+  std::vector<uint2> twh_f, twh_i;
+  std::vector<uint32_t> twl_f, twl_i;
 };
 
 // The first kMaxPrimes primes p < 2^30 with p = 1 mod 2^kPrimeLgRoot, in

@@ -105,3 +105,8 @@ def mpz_rmatrix_mult_fft(C_: MpzArray, A: MpzArray, r: int, B: MpzArray, d: int)
     w = MpzArray(n=1)
     _lib.lib().mpz_rmatrix_mult_fft(C_.ptr(), A.ptr(), r, B.ptr(), d, w.ptr())
     w.close()
+
+
+def gpu_fft_suitable(A: MpzArray, r: int, B: MpzArray, d: int) -> int:
+    """mpz_rmatrix_gpu_fft_suitable: 1 if the library can multiply these."""
+    return int(_lib.lib().mpz_rmatrix_gpu_fft_suitable(A.ptr(), r, B.ptr(), d))

@@ -58,7 +58,8 @@ def ntt_primes(count=16):
 @pytest.mark.parametrize("a_bits,b_bits,k", [
     (1, 1, 1), (64, 64, 1), (4096, 4096, 4), (65536, 65536, 8), (1 << 20, 1 << 20, 64),
     (1 << 18, 1 << 10, 16), (1 << 21, 1 << 16, 8), (300, 5, 32), (12345, 678, 3),
-    (1 << 21, 1 << 21, 2)])
+    (1 << 21, 1 << 21, 2), (1 << 23, 1 << 23, 2), (1 << 24, 1 << 24, 2),
+    (100000000, 100000000, 5), (10000000, 10000000, 5), (1 << 22, 64, 1)])
 def test_params_exactness_bound(product_lib, a_bits, b_bits, k):
     """Every product coefficient c has 4|c| < p_0...p_{P-1} (the symmetric
     CRT residue is c, with the margin the rounded explicit CRT needs) and the
@@ -71,7 +72,16 @@ def test_params_exactness_bound(product_lib, a_bits, b_bits, k):
     bound = k * min(lenA, lenB) * ((1 << r) - 1) ** 2
     assert 4 * bound < M
     assert lenA + lenB - 1 <= (1 << lg)
-    assert 2 <= P <= 16 and lg <= 15
+    assert 2 <= P <= 16 and lg <= 20
+
+
+def test_long_operands_are_suitable(product_lib):
+    """Transforms up to 2^20 points (four-step above 2^15): the operand sizes of
+    the reference's own benchmark (benchmark/bench_matmul.c: 10^7 and 10^8
+    bits, 2x2 and 5x5) all get parameters."""
+    for bits, d in [(10000000, 2), (10000000, 5), (100000000, 2), (100000000, 5)]:
+        P, r, lg = api.choose_params(bits, bits, d)
+        assert 16 <= lg <= 20
 
 
 def test_params_too_large_rejected(product_lib):
