@@ -1087,12 +1087,13 @@ struct FastDiv {
 };
 
 // One output entry by one warp: CRT of its coefficients tile by tile into
-// the warp's scratch sU (word q of tile coefficient c at [q * cmax + c]),
-// the words' sums, the carry ripple, the sign and the size.
+// the warp's scratch sV, each coefficient pre-shifted to its place in the
+// output words (P + 1 words of tile coefficient c at [c (P + 1)]), the
+// words' sums, the carry ripple, the sign and the size.
 template <int P>
 __device__ __forceinline__ void crt_entry(const InvDesc& d, const uint32_t* __restrict__ res,
                                           uint32_t* __restrict__ out,
-                                          int32_t* __restrict__ out_sizes, uint32_t* sU,
+                                          int32_t* __restrict__ out_sizes, uint32_t* sV,
                                           int cmax, int lane) {
   const unsigned FULL = 0xffffffffu;
   // bit positions fit 31 bits (an entry's words times 32 stays below 2^31),
@@ -1112,11 +1113,22 @@ __device__ __forceinline__ void crt_entry(const InvDesc& d, const uint32_t* __re
     int hi_i = (int)divr((uint32_t)(32 * (w0 + kCrtTileWords) - 1));
     if (hi_i > ncoef - 1) hi_i = ncoef - 1;
     const int ncf = hi_i >= lo_i ? hi_i - lo_i + 1 : 0;
+    // coefficient i = lo_i + c as X_i 2^(i r mod 32): P + 1 words, the top
+    // one signed (it carries the sign's borrow), so output word w adds word
+    // w - floor(i r / 32) of every coefficient that reaches it
     for (int c = lane; c < ncf; c += 32) {
       uint32_t X[P];
       crt_coeff<P>(res, d.res_off, d.lgN, lo_i + c, X);
+      const uint32_t sh = (uint32_t)((lo_i + c) * r) & 31u;
+      uint32_t* v = sV + c * (P + 1);
+      uint32_t prev = 0;
 #pragma unroll
-      for (int q = 0; q < P; ++q) sU[q * cmax + c] = X[q];
+      for (int q = 0; q < P; ++q) {
+        v[q] = sh ? ((X[q] << sh) | (prev >> (32u - sh))) : X[q];
+        prev = X[q];
+      }
+      const uint32_t fill = (uint32_t)((int32_t)X[P - 1] >> 31);
+      v[P] = sh ? ((fill << sh) | (prev >> (32u - sh))) : fill;
     }
     __syncwarp();
     for (int st = 0; st < kCrtSteps; ++st) {
@@ -1131,25 +1143,11 @@ __device__ __forceinline__ void crt_entry(const InvDesc& d, const uint32_t* __re
         }
         int ib = (int)divr((uint32_t)(32 * w + 31));
         if (ib > hi_i) ib = hi_i;
+        // 0 <= w - floor(i r / 32) <= P for every i in [ia, ib]
         for (int i = ia; i <= ib; ++i) {
-          const int c = i - lo_i;
-          const int bi = i * r;
-          const int dd = 32 * w - bi;
-          const uint32_t* U = sU + c;  // word q at U[q * cmax]
-          uint32_t slice;
-          if (dd < 0) {
-            slice = U[0] << (uint32_t)(-dd);
-          } else {
-            const int q = dd >> 5;
-            const uint32_t sh = (uint32_t)(dd & 31);
-            const uint32_t lo = q < P ? U[q * cmax] : 0u;
-            const uint32_t hi = q + 1 < P ? U[(q + 1) * cmax] : 0u;
-            slice = __funnelshift_r(lo, hi, sh);
-          }
-          sw += slice;
-          // the sign of X_i is the top bit of U_i; its borrow lands in word
-          // (i r) / 32 + P
-          if ((bi >> 5) + P == w && (U[(P - 1) * cmax] >> 31)) sw -= (int64_t)1 << (bi & 31);
+          const int q = w - ((i * r) >> 5);
+          const uint32_t x = sV[(i - lo_i) * (P + 1) + q];
+          sw += q == P ? (int64_t)(int32_t)x : (int64_t)x;
         }
       }
       const int hi = active ? (int)(sw >> 32) : 0;
@@ -1225,7 +1223,7 @@ k_crt_warp(const InvDesc* __restrict__ descs, const uint32_t* __restrict__ idx, 
   const int slot = blockIdx.x * kCrtWarps + warp;
   if (slot >= count) return;  // whole warp; no block-wide barrier below
   const InvDesc d = descs[idx[slot]];
-  crt_entry<P>(d, res, out, out_sizes, sm + warp * (cmax * P), cmax, threadIdx.x & 31);
+  crt_entry<P>(d, res, out, out_sizes, sm + warp * (cmax * (P + 1)), cmax, threadIdx.x & 31);
 }
 
 template <int P, int PHI>
@@ -1936,7 +1934,7 @@ cudaError_t launch_crt_mixed(const InvDesc* descs, const uint32_t* idx, int coun
     cs.cmax[P] = 0;
     if (P < plo || P > phi || rmin[P] <= 0) continue;
     cs.cmax[P] = crt_cmax(P, rmin[P]);
-    if (cs.cmax[P] * P > cs.warp_words) cs.warp_words = cs.cmax[P] * P;
+    if (cs.cmax[P] * (P + 1) > cs.warp_words) cs.warp_words = cs.cmax[P] * (P + 1);
   }
   if (cs.warp_words == 0) return cudaErrorInvalidValue;
   const size_t smem = sizeof(uint32_t) * (size_t)cs.warp_words * kCrtWarps;
@@ -1956,7 +1954,7 @@ static cudaError_t launch_crt_t(const InvDesc* descs, const uint32_t* idx, int c
                                 const uint32_t* res, uint32_t* out, int32_t* sizes, int rmin,
                                 cudaStream_t st) {
   const int cmax = crt_cmax(P, rmin);
-  const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * P);
+  const size_t per_warp = sizeof(uint32_t) * (size_t)(cmax * (P + 1));
   const size_t smem = per_warp * kCrtWarps;
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
   const int grid = (count + kCrtWarps - 1) / kCrtWarps;
