@@ -60,10 +60,16 @@ def parse():
     ap.add_argument("--plain-sample", type=int, default=256,
                     help="products timed one call each for the plain comparison")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
-    ap.add_argument("--serve-pool", type=int, default=96,
-                    help="distinct serving requests (config-5 draws), cycled")
-    ap.add_argument("--serve-requests", type=int, default=400,
-                    help="requests per open-loop serving run")
+    ap.add_argument("--serve-pool", type=int, default=256,
+                    help="distinct serving requests (the first config-5 draws), cycled")
+    ap.add_argument("--serve-requests", type=int, default=3000,
+                    help="requests per open-loop serving run (at most 8 s of arrivals)")
+    ap.add_argument("--serve-long", type=int, default=10000,
+                    help="requests of the long serving stream at 0.8 of saturation (0: none)")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="profiling run: build the plan, execute it --warmup times, then one "
+                         "execute between cudaProfilerStart and cudaProfilerStop (for ncu "
+                         "--profile-from-start off), and exit without a bench line")
     return ap.parse_args()
 
 
@@ -220,15 +226,29 @@ def _cpu_worker(args):
     return time.perf_counter() - t0, len(prods)
 
 
-def cpu_reference_rate(name, replicate, sample, workers, pool=None):
-    """Products/s of the reference CPU path on `sample` products, `workers`
-    processes (the reference is single-threaded)."""
+def sample_indices(name, replicate, sample, count, square):
+    """Batch products the CPU baseline times: the first `sample` of the batch,
+    or (square) the first `sample` with k == n -- the shapes the reference's
+    r x d by d x d API expresses without zero padding."""
+    if name != "config3":
+        return [0]
+    if not square:
+        return list(range(min(sample, count)))
+    from rforest_b200 import workloads as W
+    shapes = W.config3_shapes(replicate, count)
+    return [t for t, (m, k, n, bits) in enumerate(shapes) if k == n][:sample]
+
+
+def cpu_reference_rate(name, replicate, sample, workers, pool=None, square=True, count=4096):
+    """Products/s of the reference CPU path on a sample of the batch
+    (sample_indices), `workers` processes (the reference is single-threaded)."""
     from oracle import oracle as O
     kind = "reference" if O.reference_available() else None
     if kind is None:
         raise RuntimeError("oracle/_ref is not built")
-    n = sample if name == "config3" else 1
-    chunks = [list(range(i, n, workers)) for i in range(min(workers, n))]
+    idx = sample_indices(name, replicate, sample, count, square)
+    n = len(idx)
+    chunks = [idx[i::workers] for i in range(min(workers, n))]
     t0 = time.perf_counter()
     if pool is None or len(chunks) == 1:
         res = [_cpu_worker((name, replicate, c)) for c in chunks]
@@ -258,28 +278,39 @@ def run_reference_arm(args, rank, world):
     sample = args.cpu_sample
     with ctx.Pool(workers) as pool:
         for _ in range(args.warmup):
-            cpu_reference_rate(args.workload, 1, min(sample, workers), workers, pool)
+            cpu_reference_rate(args.workload, 1, min(sample, workers), workers, pool,
+                               count=args.count)
         rates = []
         t0 = time.perf_counter()
         done_total = 0
         for _ in range(args.steps):
-            rate, used, done = cpu_reference_rate(args.workload, 1, sample, workers, pool)
+            rate, used, done = cpu_reference_rate(args.workload, 1, sample, workers, pool,
+                                                  count=args.count)
             rates.append(rate)
             done_total += done
         wall = time.perf_counter() - t0
+        # informative: the first products of the batch whatever their shape,
+        # zero-padded to d = max(k, n) for the reference's API
+        padded, _, padded_done = cpu_reference_rate(args.workload, 1, sample, workers, pool,
+                                                    square=False, count=args.count)
     value = done_total / wall
     cfg = workload_config(args.workload, args.count)
+    sample_note = (f"the first {done_total // max(1, args.steps)} products of the batch with "
+                   f"k == n per step (the reference's r x d by d x d API takes them unpadded), "
+                   f"{used} worker processes")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": dict(cfg, sample_products_per_step=sample if args.workload == "config3" else 1,
-                       cpu_note="reference API is r x d by d x d: shapes zero-padded to "
-                                "d = max(k, n)"),
+        "config": dict(cfg, sample_products_per_step=done_total // max(1, args.steps),
+                       cpu_note="sample restricted to k == n products, which the reference's "
+                                "r x d by d x d API multiplies without zero padding"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference",
-                         "sample": f"first {sample} products of the batch per step, "
-                                   f"{used} worker processes"},
+                         "sample": sample_note,
+                         "padded": {"value": padded, "unit": UNIT,
+                                    "sample": f"first {padded_done} products of the batch, "
+                                              f"zero-padded to d = max(k, n)"}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -323,6 +354,19 @@ def main():
     # ---- device-resident throughput ----
     plan = api.Plan(triples, stream=stream)
     info = plan.info(0)
+    if args.profile_step:
+        for _ in range(args.warmup):
+            plan.execute(stream)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        plan.execute(stream)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_step": args.workload, "products": len(triples),
+                          "launches_per_execute": info["launches"],
+                          "device_bytes": info["device_bytes"]}), flush=True)
+        plan.close()
+        return
     for _ in range(args.warmup):
         plan.execute(stream)
     stream.synchronize()
@@ -414,6 +458,7 @@ def main():
         comparisons = compare_forms(api, torch, stream, triples, args)
         api.set_contract_mode(modes[args.contract])
         comparisons["mod_reduction"] = mod_benchmark(api)
+        comparisons["config4"] = config4_benchmark(api, torch, stream)
 
     if rank == 0:
         # roofline of the dominant stage (3-pass model, reference parameters)
@@ -427,23 +472,26 @@ def main():
         else:
             alg, t_ms, kern, stage = (b3, stage_ms[2] + stage_ms[3], "k_inv2+k_crt_mixed",
                                       "inv_crt")
-        # DRAM bytes per step of the stage on the 4096-product batch: ncu
-        # (dram__bytes_read.sum + dram__bytes_write.sum) on the 512-product
-        # step, scaled by the batch's residue points (x7.81 forward, x7.50
-        # contraction); profiles/ has the captures
-        traffic = None
-        if args.workload == "config3" and args.count == 4096:
-            traffic = {"fwd": 19.5e9, "contract": 32.9e9}.get(stage)
+        # DRAM bytes per step of the stage: the committed ncu summary of the
+        # same workload (dram__bytes_read.sum + dram__bytes_write.sum per
+        # kernel of one step, profiles/dram_traffic_config3.txt)
+        traffic, traffic_src = load_traffic(args.workload, args.count, stage)
         peaks = load_peaks()
         per_launch_s = (t_ms / 1000.0) / max(1, timed)
         achieved = alg / per_launch_s / 1e9
         cpu = None
         if cpu_pool is not None:
             rate, used, done = cpu_reference_rate(args.workload, 1, args.cpu_sample, workers,
-                                                  cpu_pool)
+                                                  cpu_pool, count=args.count)
+            prate, _, pdone = cpu_reference_rate(args.workload, 1, args.cpu_sample, workers,
+                                                 cpu_pool, square=False, count=args.count)
             cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "reference",
-                   "sample": f"first {done} products of the batch, reference CPU "
-                             f"mpz_rmatrix_mult_fft, {used} worker processes"}
+                   "sample": f"the first {done} products of the batch with k == n (the "
+                             f"reference's r x d by d x d API takes them unpadded), reference "
+                             f"CPU mpz_rmatrix_mult_fft, {used} worker processes",
+                   "padded": {"value": prate, "unit": UNIT,
+                              "sample": f"first {pdone} products of the batch, zero-padded "
+                                        f"to d = max(k, n)"}}
             cpu_pool.close()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -475,8 +523,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved,
                          "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
                          "peak_source": peaks[1], "traffic": traffic,
-                         "traffic_note": "DRAM bytes per step (ncu, 512-product step scaled)"
-                         if traffic else None,
+                         "traffic_note": traffic_src,
                          "alg_bytes_per_step": alg,
                          "alg_note": "3-pass byte model at the reference's parameters "
                                      "(4 primes, u64 residues)"},
@@ -556,6 +603,43 @@ def compare_forms(api, torch, stream, triples, args):
     return out
 
 
+def config4_benchmark(api, torch, stream, reps=3):
+    """The large dense contraction (config 4: 64x64 by 64x64, unsigned 2^20-bit
+    entries) device-resident, per stage, on CUDA cores and on tensor cores;
+    each engine's result checked against the reference's golden digest."""
+    from rforest_b200 import packed as PK, workloads as W
+    p = W.config4()
+    want = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "digests.json")) as f:
+            want = json.load(f)["config4"]["C"]
+    except (OSError, KeyError, ValueError):
+        pass
+    saved = api.contract_mode()
+    names = ["split_fwd_ntt", "contract", "inv_ntt", "crt_recompose"]
+    out = {"workload": "64x64 by 64x64, unsigned 2^20-bit entries", "reps": reps}
+    try:
+        for label, mode in (("cuda_cores", 1), ("tensor_cores", 2)):
+            api.set_contract_mode(mode)
+            plan = api.Plan([(p.m, p.k, p.n, p.A, p.B)], stream=stream)
+            plan.execute(stream)
+            plan.set_timing(True)
+            for _ in range(reps):
+                plan.execute(stream)
+            stage_ms, _, timed = plan.stage_times()
+            plan.set_timing(False)
+            C = plan.download(stream)[0]
+            out[label] = {"ms_per_product": round(sum(stage_ms) / max(1, timed), 3),
+                          "stages_ms": {n: round(t / max(1, timed), 3)
+                                        for n, t in zip(names, stage_ms)},
+                          "verified": None if want is None else PK.digest(C) == want}
+            out["params"] = plan.info(0)
+            plan.close()
+    finally:
+        api.set_contract_mode(saved)
+    return out
+
+
 def mod_benchmark(api):
     """x mod d beside the product (a remainder-tree step): 2048 signed x of
     2^17 bits by one d of 2^16 bits, through mpzmm_mod_batch (host arrays in,
@@ -606,14 +690,23 @@ def serving_benchmark(api, args):
     """Open-loop serving of config-5 requests (m,k,n uniform in 2..32, entry
     bit lengths log-uniform in [2^8, 2^20], signed) through the continuous-
     batching server: saturation throughput, then Poisson arrivals at 0.5, 0.8
-    and 0.95 of it with p50/p99 latency (submit to result in host memory).
-    A pool of distinct seeded requests is cycled to bound host memory."""
+    and 0.95 of it with p50/p99 latency (submit to result in host memory),
+    and one long stream.  The requests are the first `serve_pool` of the
+    config-5 stream -- the ones whose results the reference computed for the
+    golden digests -- cycled to bound host memory; the first served pass of
+    the pool is checked against those digests."""
     import threading
-    from rforest_b200 import workloads as W
+    from rforest_b200 import packed as PK, workloads as W
     pool = [W.config5_request(1, t) for t in range(args.serve_pool)]
     trip = [(p.m, p.k, p.n, p.A, p.B) for p in pool]
     out = {"workload": "config-5 requests: m,k,n uniform in {2..32}, bits log-uniform "
                        "[2^8, 2^20], signed", "pool": len(pool)}
+    want = None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "digests.json")) as f:
+            want = json.load(f)["config5"]["C"]
+    except (OSError, KeyError, ValueError):
+        pass
     # plain GPU path: one call per request over the whole pool, no batching;
     # a first pass grows the library's workspace, as the server's warm-up does
     for t in trip:
@@ -621,20 +714,34 @@ def serving_benchmark(api, args):
     t0 = time.perf_counter()
     for t in trip:
         api.matmul(*t)
-    out["plain_one_call_per_request"] = {"value": len(trip) / (time.perf_counter() - t0),
-                                         "unit": "requests/s",
+    plain = len(trip) / (time.perf_counter() - t0)
+    out["plain_one_call_per_request"] = {"value": plain, "unit": "requests/s",
                                          "note": "mpzmm_matmul per request, same pool"}
-    srv = api.Server(slots=3, max_batch=32)
-    out["server_config"] = {"slots": 3, "max_batch": 32, "budget": "3/4 of free memory"}
+    slots, max_batch, window = 3, 32, 200
+    srv = api.Server(slots=slots, max_batch=max_batch, window_us=window)
+    out["server_config"] = {"slots": slots, "max_batch": max_batch, "window_us": window,
+                            "budget": "3/4 of free memory"}
     try:
-        # warm-up: two passes of the pool grow every slot's pinned staging and
-        # the device memory pool, so the timed runs measure steady state
-        tickets = [srv.submit(*trip[i % len(trip)]) for i in range(2 * len(trip))]
+        # first pass: every pool request once, all queued; results checked
+        tickets = [srv.submit(*t) for t in trip]
+        checked = 0
+        bad = 0
+        for i, t in enumerate(tickets):
+            C = srv.wait(t, 600000)
+            if want is not None and i < len(want):
+                checked += 1
+                bad += PK.digest(C) != want[i]
+            srv.release(t)
+        out["verified"] = {"checked": checked, "mismatches": bad,
+                           "against": "reference digests of config-5 requests 0..255"}
+        # warm-up: another pass grows every slot's pinned staging and workspace
+        tickets = [srv.submit(*trip[i % len(trip)]) for i in range(len(trip))]
         for t in tickets:
             srv.wait(t, 600000)
             srv.release(t)
         # saturation: everything queued at once
-        nsat = max(len(trip), 2 * len(trip))
+        st0 = srv.stats()
+        nsat = 2 * len(trip)
         t0 = time.perf_counter()
         tickets = [srv.submit(*trip[i % len(trip)]) for i in range(nsat)]
         for t in tickets:
@@ -642,11 +749,12 @@ def serving_benchmark(api, args):
         sat = nsat / (time.perf_counter() - t0)
         for t in tickets:
             srv.release(t)
-        out["saturation"] = {"value": sat, "unit": "requests/s"}
-        runs = []
-        for frac in (0.5, 0.8, 0.95):
-            lam = frac * sat
-            R = int(max(64, min(args.serve_requests, lam * 6.0)))
+        st1 = srv.stats()
+        out["saturation"] = {"value": sat, "unit": "requests/s", "requests": nsat,
+                             "vs_plain": sat / plain,
+                             "products_per_batch": nsat / max(1, st1["batches"] - st0["batches"])}
+
+        def stream(lam, R):
             arr = W.poisson_arrivals(1, R, lam)
             tickets = [None] * R
 
@@ -658,27 +766,56 @@ def serving_benchmark(api, args):
                         time.sleep(delay)
                     tickets[i] = srv.submit(*trip[i % len(trip)])
 
+            b0 = srv.stats()["batches"]
             th = threading.Thread(target=feeder)
             th.start()
-            th.join()
             lat, subs, dones = [], [], []
-            for t in tickets:
-                srv.wait(t, 600000)
-                s0, _, d0 = srv.times(t)
+            for i in range(R):
+                while tickets[i] is None:
+                    time.sleep(0.0002)
+                srv.wait(tickets[i], 600000)
+                s0, _, d0 = srv.times(tickets[i])
                 lat.append((d0 - s0) / 1e6)
                 subs.append(s0)
                 dones.append(d0)
-                srv.release(t)
+                srv.release(tickets[i])
+            th.join()
             span = (max(dones) - min(subs)) / 1e9
-            runs.append({"load": frac, "offered": lam, "requests": R,
-                         "throughput": R / span, "p50_ms": _pct(lat, 50),
-                         "p99_ms": _pct(lat, 99), "unit": "requests/s"})
+            return {"offered": lam, "requests": R, "throughput": R / span,
+                    "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "unit": "requests/s",
+                    "products_per_batch": R / max(1, srv.stats()["batches"] - b0)}
+
+        runs = []
+        for frac in (0.5, 0.8, 0.95):
+            lam = frac * sat
+            R = int(max(256, min(args.serve_requests, lam * 8.0)))
+            runs.append(dict(load=frac, **stream(lam, R)))
         out["runs"] = runs
+        if args.serve_long > 0:
+            out["long_stream"] = dict(load=0.8, **stream(0.8 * sat, args.serve_long))
         out["server"] = srv.stats()
         out["server_phase_ms"] = srv.phase_ms()
     finally:
         srv.close()
     return out
+
+
+def load_traffic(name, count, stage):
+    """DRAM bytes per step of a stage from the committed ncu summary of this
+    workload (a JSON object in profiles/dram_traffic_<workload>.txt with the
+    capture's command); (None, why) where there is none."""
+    path = os.path.join(ROOT, "profiles", f"dram_traffic_{name}.txt")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return None, "no ncu DRAM summary committed for this workload"
+    if int(d.get("products_per_step", -1)) != count:
+        return None, f"ncu DRAM summary is for {d.get('products_per_step')} products a step"
+    v = d.get("bytes_per_step", {}).get(stage)
+    if v is None:
+        return None, f"ncu DRAM summary has no '{stage}' stage"
+    return float(v), f"DRAM bytes per step (ncu, {os.path.basename(path)}: {d.get('captured', '')})"
 
 
 def load_peaks():

@@ -365,6 +365,12 @@ MPZMM_API int mpzmm_server_stats(mpzmm_server *server, int64_t *batches, int64_t
 /* Scheduler-thread nanoseconds spent in: plan building, input gather and
    copy, kernel launches, result copy-back and scatter (4 values). */
 MPZMM_API int mpzmm_server_phase_ns(mpzmm_server *server, int64_t *ns4);
+/* Admission window: when a slot frees up while other batches are on the GPU,
+   it keeps admitting queued requests for up to this many microseconds
+   before launching its batch (default 200; 0 launches at once).  With the
+   GPU idle a batch always launches at once.  Larger batches at load, at the
+   cost of at most the window in latency. */
+MPZMM_API int mpzmm_server_set_admission_window(mpzmm_server *server, int64_t microseconds);
 /* Finishes queued and in-flight work, then frees the server. */
 MPZMM_API void mpzmm_server_destroy(mpzmm_server *server);
 

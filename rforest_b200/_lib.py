@@ -108,6 +108,7 @@ def lib():
         "mpzmm_server_ticket_times": (C.c_int, [vp, C.c_uint64, i64p, i64p, i64p]),
         "mpzmm_server_release": (C.c_int, [vp, C.c_uint64]),
         "mpzmm_server_stats": (C.c_int, [vp, i64p, i64p, i64p]),
+        "mpzmm_server_set_admission_window": (C.c_int, [vp, C.c_int64]),
         "mpzmm_server_destroy": (None, [vp]),
         "mpzmm_server_phase_ns": (C.c_int, [vp, i64p]),
         "mpzmm_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),

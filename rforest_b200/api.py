@@ -400,11 +400,17 @@ class Plan:
 class Server:
     """Continuous-batching request server (mpzmm_server_* of the C ABI)."""
 
-    def __init__(self, budget_bytes: int = 0, slots: int = 3, max_batch: int = 0):
+    def __init__(self, budget_bytes: int = 0, slots: int = 3, max_batch: int = 0,
+                 window_us: Optional[int] = None):
         self.handle = C.c_void_p()
         _lib.check(_lib.lib().mpzmm_server_create(C.byref(self.handle), budget_bytes, slots,
                                                   max_batch))
         self.holders = {}
+        if window_us is not None:
+            self.set_admission_window(window_us)
+
+    def set_admission_window(self, microseconds: int) -> None:
+        _lib.check(_lib.lib().mpzmm_server_set_admission_window(self.handle, int(microseconds)))
 
     def submit(self, m: int, k: int, n: int, A: Packed, B: Packed) -> int:
         h = _Holder(m, k, n, A, B)

@@ -327,6 +327,8 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
     if (take_test_fail_alloc())
       return set_error(kErrNoMem, "injected device allocation failure (test option)");
     auto alloc = [&](size_t count) {
+      if (async_stream && pool)
+        return cudaMallocFromPoolAsync((void**)p, count * elem, pool, async_stream);
       return async_stream ? cudaMallocAsync((void**)p, count * elem, async_stream)
                           : cudaMalloc((void**)p, count * elem);
     };
@@ -370,8 +372,11 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   if ((st = grow_dev(&d_sizes, cap_sizes, sizes, 4))) return st;
   if ((st = grow_dev(&d_desc, cap_desc, desc_bytes, 1))) return st;
   if (!d_status) {
-    cudaError_t e = async_stream ? cudaMallocAsync((void**)&d_status, sizeof(int), async_stream)
-                                 : cudaMalloc((void**)&d_status, sizeof(int));
+    cudaError_t e =
+        async_stream
+            ? (pool ? cudaMallocFromPoolAsync((void**)&d_status, sizeof(int), pool, async_stream)
+                    : cudaMallocAsync((void**)&d_status, sizeof(int), async_stream))
+            : cudaMalloc((void**)&d_status, sizeof(int));
     if (e != cudaSuccess) {
       d_status = nullptr;
       return set_error(kErrNoMem, std::string("cudaMalloc(status): ") + cudaGetErrorString(e));

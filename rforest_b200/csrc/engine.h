@@ -92,9 +92,11 @@ struct Workspace {
   size_t cap_limbs = 0, cap_res = 0, cap_out = 0, cap_sizes = 0, cap_desc = 0;
   size_t hcap_limbs = 0, hcap_out = 0, hcap_sizes = 0, hcap_desc = 0;
   int64_t device_bytes = 0;
-  // With a stream set, device buffers come from the stream-ordered memory
-  // pool (cudaMallocAsync / cudaFreeAsync on that stream).
+  // With a stream set, device buffers come from a stream-ordered memory pool
+  // (cudaMallocAsync / cudaFreeAsync on that stream): `pool` if set, else
+  // the device's default pool.  Nothing then synchronises the device.
   cudaStream_t async_stream = nullptr;
+  cudaMemPool_t pool = nullptr;
   // Ensures room for the given element counts (device buffers, then the
   // pinned staging of limbs and output words); returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,

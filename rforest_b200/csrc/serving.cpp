@@ -56,6 +56,13 @@ struct mpzmm_server {
   int64_t budget = 0;
   int max_batch = 0;
   int device = 0;
+  // admission window: a slot that frees up while other batches occupy the
+  // GPU keeps admitting for up to this long before it launches (ns)
+  int64_t window_ns = 200000;
+  // device memory of the slots' workspaces: a stream-ordered pool of the
+  // server's own that keeps freed memory, so a workspace growing or being
+  // released never synchronises the device or stalls the other slots
+  cudaMemPool_t pool = nullptr;
   std::vector<std::unique_ptr<Slot>> slots;
   std::mutex mu;
   std::condition_variable cv_work;  // slots wake up: new request, freed budget, stop
@@ -66,6 +73,7 @@ struct mpzmm_server {
   bool stop = false;
   int64_t in_flight_bytes = 0;
   int64_t stat_batches = 0, stat_products = 0, stat_max_in_flight = 0;
+  int64_t stat_batched_products = 0;  // products admitted into launched batches
   // slot-thread time per phase, summed over slots (ns): plan build, input
   // gather + copy, launches, wait + result copy-back + scatter
   int64_t ns_build = 0, ns_upload = 0, ns_launch = 0, ns_download = 0;
@@ -139,9 +147,27 @@ struct mpzmm_server {
           if (stop && queue.empty()) return;
           cv_work.wait(lk);
         }
+        int others = 0;
+        for (auto& o : slots) others += o->busy ? 1 : 0;
         s.busy = true;
         in_flight_bytes += bytes;
+        // the GPU is busy with other batches anyway: let this batch fill for
+        // a bounded window (an idle GPU gets the batch at once)
+        auto full = [&] { return max_batch > 0 && (int)batch.size() >= max_batch; };
+        if (others > 0 && window_ns > 0 && !full()) {
+          const auto deadline =
+              std::chrono::steady_clock::now() + std::chrono::nanoseconds(window_ns);
+          for (;;) {
+            const bool timed_out = cv_work.wait_until(lk, deadline) == std::cv_status::timeout;
+            int64_t more = 0;
+            admit(batch, more);
+            in_flight_bytes += more;
+            bytes += more;
+            if (timed_out || full() || stop) break;
+          }
+        }
         ++stat_batches;
+        stat_batched_products += (int64_t)batch.size();
         int in_flight = 0;
         for (auto& o : slots) in_flight += o->busy ? 1 : 0;
         if (in_flight > stat_max_in_flight) stat_max_in_flight = in_flight;
@@ -182,13 +208,32 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
   s->budget = budget_bytes;
   s->max_batch = max_batch;
   s->device = context().device;
+  {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+    if (e != cudaSuccess) return set_error(kErrCuda, std::string("cudaMemPoolCreate: ") +
+                                                         cudaGetErrorString(e));
+    uint64_t keep = ~(uint64_t)0;  // freed memory stays in the pool
+    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(s->pool);
+      return set_error(kErrCuda, std::string("cudaMemPoolSetAttribute: ") +
+                                     cudaGetErrorString(e));
+    }
+  }
   for (int i = 0; i < slots; ++i) {
     std::unique_ptr<Slot> sl(new Slot);
     cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
       for (auto& o : s->slots) cudaStreamDestroy(o->stream);
+      cudaMemPoolDestroy(s->pool);
       return set_error(kErrCuda, cudaGetErrorString(e));
     }
+    sl->ws.async_stream = sl->stream;
+    sl->ws.pool = s->pool;
     s->slots.push_back(std::move(sl));
   }
   mpzmm_server* raw = s.get();
@@ -294,6 +339,14 @@ int mpzmm_server_phase_ns(mpzmm_server* s, int64_t* ns4) {
   return kOk;
 }
 
+int mpzmm_server_set_admission_window(mpzmm_server* s, int64_t microseconds) {
+  if (!s) return set_error(kErrArg, "null server");
+  if (microseconds < 0) return set_error(kErrArg, "window must be >= 0");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->window_ns = microseconds * 1000;
+  return kOk;
+}
+
 int mpzmm_server_stats(mpzmm_server* s, int64_t* batches, int64_t* products,
                        int64_t* max_in_flight) {
   if (!s) return set_error(kErrArg, "null server");
@@ -315,9 +368,11 @@ void mpzmm_server_destroy(mpzmm_server* s) {
     if (sl->thread.joinable()) sl->thread.join();
   for (auto& sl : s->slots) {
     cudaStreamSynchronize(sl->stream);
-    sl->ws.release();
+    sl->ws.release();  // stream-ordered frees on the slot's stream
+    cudaStreamSynchronize(sl->stream);
     cudaStreamDestroy(sl->stream);
   }
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
 }
 
