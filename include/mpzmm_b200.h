@@ -164,11 +164,12 @@ MPZMM_API int mpzmm_batch_timeline(double *rows, int max_chunks, int *nchunks);
 MPZMM_API int mpzmm_batch_chunks(int count, const int64_t *limbs, int64_t chunk_limbs,
                                  int64_t *bounds, int max_bounds, int *nchunks);
 
-/* Autotuner: times the contraction of a representative product per size
+/* Autotuner: times the contraction of a representative batch per size
    class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
-   entries) on CUDA cores and on tensor cores and makes automatic mode use
-   tensor cores for that class where they took under 3/4 of the CUDA-core
-   time (until then automatic mode uses CUDA cores).  ms_out, if not NULL, receives 40 floats: {CUDA, tensor}
+   entries, copies of one product until every SM has several blocks' work)
+   on CUDA cores and on tensor cores and makes automatic mode use tensor
+   cores for that class where they took under 3/4 of the CUDA-core time
+   (until then automatic mode uses CUDA cores).  ms_out, if not NULL, receives 40 floats: {CUDA, tensor}
    milliseconds per class, k-major. */
 MPZMM_API int mpzmm_autotune(void *stream, float *ms_out);
 
@@ -335,13 +336,16 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
 /* ---- continuous-batching server (no counterpart in the reference) ----
    Up to `slots` batches are in flight, each slot with its own host thread,
    CUDA stream and workspace.  Whenever a slot is free it admits queued
-   requests in arrival
-   order into one batch while their estimated device footprint fits what the
-   in-flight batches leave of `budget_bytes` (0: three quarters of the free
-   device memory), with at most `max_batch` products per batch (0: no
-   limit).  Requests that arrive while batches run join the next batch; a
-   request's residues stay on the device for the whole pipeline.  A request
-   larger than the budget is refused (MPZMM_ERR_TOO_LARGE). */
+   requests in arrival order into one batch while their estimated device
+   footprint fits what the in-flight batches leave of `budget_bytes` (0:
+   three quarters of the free device memory), with at most `max_batch`
+   products per batch (0: no limit) and at most 256 MB of inputs and outputs
+   (a larger request is a batch of its own).  Requests that arrive while
+   batches run join the next batch; a request's residues stay on the device
+   for the whole pipeline.  Each slot's pinned staging is allocated once at
+   creation and its device memory comes from a stream-ordered pool of the
+   server's own, so no batch synchronises the device.  A request larger than
+   the budget is refused (MPZMM_ERR_TOO_LARGE). */
 typedef struct mpzmm_server mpzmm_server;
 MPZMM_API int mpzmm_server_create(mpzmm_server **server, int64_t budget_bytes, int slots,
                                   int max_batch);

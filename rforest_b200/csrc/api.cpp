@@ -136,10 +136,10 @@ int mpzmm_set_option(int option, int value) {
   return set_error(kErrArg, "unknown option");
 }
 
-// Times the contraction stage of one representative product per size class
-// (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit entries) on
-// CUDA cores and on tensor cores, and records the faster engine for
-// automatic mode.  ms_out (optional) receives {cuda, tc} milliseconds per
+// Times the contraction stage of a representative batch per size class
+// (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit entries,
+// copies of one product until the GPU is full) on CUDA cores and on tensor
+// cores, and records the faster engine for automatic mode.  ms_out (optional) receives {cuda, tc} milliseconds per
 // class, k-major (40 floats).
 int mpzmm_autotune(void* stream, float* ms_out) {
   int st = ensure_setup(-1);
@@ -165,21 +165,33 @@ int mpzmm_autotune(void* stream, float* ms_out) {
       }
       const int cap = 2 * nl + 2;
       std::vector<uint64_t> out((size_t)m * n * cap);
+      // the probe runs at load: copies of the product (sharing the host
+      // arrays) until either engine has about eight CTAs' work per SM -- a
+      // single small product leaves most of the GPU idle and favours
+      // whichever engine does more per CTA, which is not what a batch sees
+      Params prm;
+      if (!choose_params(64 * nl, 64 * nl, m, k, n, &prm)) return fail(kErrTooLarge);
+      const int64_t ctas = (int64_t)prm.P * (((int64_t)1 << prm.lgN) + 127) / 128;
+      int64_t copies = (8 * (int64_t)context().num_sms + ctas - 1) / (ctas > 0 ? ctas : 1);
+      if (copies < 1) copies = 1;
+      if (copies > 256) copies = 256;
       float ms[2] = {0.f, 0.f};
       for (int mode = 1; mode <= 2; ++mode) {
-        ProductSpec ps;
-        ps.m = m;
-        ps.k = k;
-        ps.n = n;
-        for (int e = 0; e < m * k; ++e) ps.a.push_back(EntryRef{&limbs[(size_t)e * nl], nl});
-        for (int e = 0; e < k * n; ++e)
-          ps.b.push_back(EntryRef{&limbs[(size_t)(m * k + e) * nl], nl});
-        for (int e = 0; e < m * n; ++e)
-          ps.c.push_back(OutRef{&out[(size_t)e * cap], cap, nullptr, nullptr});
+        std::vector<ProductSpec> v;
+        for (int64_t c = 0; c < copies; ++c) {
+          ProductSpec ps;
+          ps.m = m;
+          ps.k = k;
+          ps.n = n;
+          for (int e = 0; e < m * k; ++e) ps.a.push_back(EntryRef{&limbs[(size_t)e * nl], nl});
+          for (int e = 0; e < k * n; ++e)
+            ps.b.push_back(EntryRef{&limbs[(size_t)(m * k + e) * nl], nl});
+          for (int e = 0; e < m * n; ++e)
+            ps.c.push_back(OutRef{&out[(size_t)e * cap], cap, nullptr, nullptr});
+          v.push_back(std::move(ps));
+        }
         context().contract_mode = mode;
         Plan plan;
-        std::vector<ProductSpec> v;
-        v.push_back(std::move(ps));
         if ((st = plan.build(std::move(v))) || (st = plan.upload(s)) || (st = plan.execute(s)))
           return fail(st);
         // fastest of five timed executes: one slow repeat (another process
@@ -195,10 +207,8 @@ int mpzmm_autotune(void* stream, float* ms_out) {
         }
         ms[mode - 1] = best < 0.f ? 0.f : best;
       }
-      // tensor cores only with a clear margin: the probe is one product, and
-      // in a large batch the tensor-core kernel's per-block set-up weighs
-      // more than it does here (a near tie measured on one product turned
-      // into a 20x slower contraction of the 4096-product batch)
+      // tensor cores only with a clear margin (a near tie measured on a
+      // probe once turned into a far slower contraction of a real batch)
       context().tc_pref[bk][bm] = ms[1] < 0.75f * ms[0] ? 1 : 0;
       if (ms_out) {
         ms_out[2 * (bk * 5 + bm)] = ms[0];

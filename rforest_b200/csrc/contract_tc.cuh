@@ -17,14 +17,15 @@
 // Montgomery-reduces it, so C carries the same 2^-32 factor as the CUDA-core
 // contraction.
 //
-// One CTA of 256 threads per (product, prime, block of 16 frequencies),
+// One CTA of 256 threads per (product, prime, block of 128 frequencies),
 // processed F frequencies at a time: all warps stage A' and B' of the F
 // frequencies straight from global memory (F consecutive residues of a
 // polynomial per vector load) into canonical K-major no-swizzle tiles (8-row
 // x 16-byte core matrices; every st.shared of a warp hits 32 distinct
-// banks); one thread issues the MMAs of a unit (one frequency, up to 32 of
-// its output columns), tcgen05.commit arrives on the unit's mbarrier; with two
-// TMEM accumulators the next unit's MMAs run while all eight warps drain the
+// banks); one thread issues the MMAs of a unit (several frequencies of a
+// product with at most 32 output columns, else one frequency's 32 columns),
+// tcgen05.commit arrives on the unit's mbarrier; with two 256-column TMEM
+// buffers the next unit's MMAs run while all eight warps drain the
 // current one (warp w reads TMEM lanes 32 (w mod 4) .. + 31, the two
 // warpgroups take alternate 16-column chunks).  Results of the F
 // frequencies are gathered in shared memory and stored F residues per vector
@@ -42,7 +43,7 @@ constexpr int kThreads = 256;
 constexpr int kMaxK = 64;        // k <= 64: K' = k bytes padded to 32, z < 2^57
 constexpr int kMaxN = 64;        // n <= 64: at most two units of 32 outputs a frequency
 constexpr int kMaxM = 128;       // m <= 128: four planes in four 128-lane tiles
-constexpr int kFreqs = 16;       // frequencies per CTA
+constexpr int kFreqs = 128;      // frequencies per CTA (each polynomial's 512 bytes)
 constexpr int kUnitCols = 32;    // output columns l per unit
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // one second of wall time
@@ -81,22 +82,21 @@ __host__ __device__ inline Shape shape_of(int m, int k, int n) {
   return s;
 }
 
-// TMEM columns of one accumulator (a unit) and whether two fit.
+// TMEM columns of one frequency's accumulator (one column range).
 __host__ __device__ inline int unit_cols(const Shape& s) { return s.mt * s.ncol; }
-__host__ __device__ inline bool double_buffered(const Shape& s) { return 2 * unit_cols(s) <= 512; }
 
-// Dynamic shared memory of a CTA for F frequencies at a time.
-__host__ __device__ inline int smem_bytes(const Shape& s, int m, int n, int F) {
-  const int out = ((m * n * F * 4) + 15) & ~15;
-  return F * (s.a_bytes + s.b_bytes) + s.red_bytes + out;
-}
+// A launch keeps two accumulator buffers of `bufcols` TMEM columns (a power
+// of two at least as wide as its widest product's accumulator) when both fit
+// the 512 columns of an SM, one otherwise.
+__host__ __device__ inline bool double_buffered(int bufcols) { return 2 * bufcols <= 512; }
 
-// TMEM columns to allocate: a power of two >= 32.
-__host__ __device__ inline int tmem_alloc_cols(const Shape& s) {
-  const int need = (double_buffered(s) ? 2 : 1) * unit_cols(s);
-  int c = 32;
-  while (c < need) c <<= 1;
-  return c;
+// Frequencies per unit when F are staged: products with one column range
+// (n <= 32) put that many frequencies' accumulators side by side in a
+// buffer, so one commit and one epilogue pass serve them all.
+__host__ __device__ inline int group_freqs(const Shape& s, int F, int bufcols) {
+  if (s.nunits != 1) return 1;
+  int g = bufcols / unit_cols(s);
+  return g < 1 ? 1 : (g > F ? F : g);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -430,7 +430,7 @@ void Workspace::release() {
   hcap_limbs = hcap_out = hcap_sizes = hcap_desc = 0;
 }
 
-int64_t estimate_device_bytes(const ProductSpec& ps) {
+int64_t estimate_device_bytes(const ProductSpec& ps, int64_t* host_bytes) {
   int64_t a_bits = 0, b_bits = 0, limbs = 0;
   for (const auto& e : ps.a) {
     const int64_t b = bit_length(e);
@@ -448,7 +448,31 @@ int64_t estimate_device_bytes(const ProductSpec& ps) {
   const int64_t res = prm.P ? entries * prm.P * ((int64_t)1 << prm.lgN) * 4 : 0;
   const int64_t out = (int64_t)ps.m * ps.n * prm.out_limbs * 8;
   const int64_t desc = entries * 64 + 4096;
+  if (host_bytes) *host_bytes = limbs * 8 + out;
   return limbs * 8 + res + out + desc;
+}
+
+int Workspace::reserve_staging(size_t stage_limbs, size_t stage_out_words) {
+  auto grow = [](auto** p, size_t& cap, size_t want, size_t elem) -> int {
+    if (want <= cap) return kOk;
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    cap = 0;
+    if (take_test_fail_alloc())
+      return set_error(kErrNoMem, "injected pinned-host allocation failure (test option)");
+    const cudaError_t e = cudaMallocHost((void**)p, want * elem);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      return set_error(kErrNoMem, std::string("cudaMallocHost of ") +
+                                      std::to_string(want * elem) + " bytes: " +
+                                      cudaGetErrorString(e));
+    }
+    cap = want;
+    return kOk;
+  };
+  int st = grow(&h_limbs, hcap_limbs, stage_limbs, 8);
+  if (!st) st = grow(&h_out, hcap_out, stage_out_words, 4);
+  return st;
 }
 
 // Checks one product, finds its operands' bit lengths and its transform
@@ -657,9 +681,10 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     const bool use_tc = contract_tc_eligible(m, k, n) &&
                         (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)][tc_bucket_mn(m, n)] == 1));
     if (use_tc) {
-      if (m > tc_max_m_) tc_max_m_ = m;
-      if (k > tc_max_k_) tc_max_k_ = k;
-      if (n > tc_max_n_) tc_max_n_ = n;
+      bool seen = false;
+      for (size_t q = 0; q < tc_shapes_.size() && !seen; q += 3)
+        seen = tc_shapes_[q] == m && tc_shapes_[q + 1] == k && tc_shapes_[q + 2] == n;
+      if (!seen) tc_shapes_.insert(tc_shapes_.end(), {m, k, n});
     }
     const uint64_t fstep = use_tc ? (uint64_t)kTcFreqsPerCta : (uint64_t)block_freqs;
     for (int j = 0; j < P; ++j)
@@ -1020,8 +1045,9 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
   if (!tc_items_.empty())
-    CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res, tc_max_m_,
-                          tc_max_k_, tc_max_n_, ws_->d_status, st, take_test_stall_tc() ? 1 : 0),
+    CU(launch_contract_tc(d_pd_, d_tc_items_, (int)tc_items_.size(), ws_->d_res,
+                          tc_shapes_.data(), (int)(tc_shapes_.size() / 3), ws_->d_status, st,
+                          take_test_stall_tc() ? 1 : 0),
        "tensor-core contraction launch");
   if (timed) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
   for (const Group& g : inv_groups_) {

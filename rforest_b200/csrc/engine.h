@@ -101,14 +101,20 @@ struct Workspace {
   // pinned staging of limbs and output words); returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,
               size_t stage_limbs, size_t stage_out_words);
+  // Grows only the pinned staging (limbs, output words) to at least these
+  // counts: a long-lived workspace sized once so that later batches never
+  // allocate pinned memory (cudaMallocHost is slow and cudaFreeHost
+  // synchronises the device).
+  int reserve_staging(size_t stage_limbs, size_t stage_out_words);
   void release_device();  // device buffers only (pinned host buffers stay)
   void release();
   ~Workspace() { release(); }
 };
 
 // Device bytes a batch of products will reserve (parameters, residues,
-// limbs, outputs and descriptors), without building it.
-int64_t estimate_device_bytes(const ProductSpec& ps);
+// limbs, outputs and descriptors), without building it; host_bytes (if
+// given) receives the bytes its inputs and outputs move across the link.
+int64_t estimate_device_bytes(const ProductSpec& ps, int64_t* host_bytes = nullptr);
 
 // Process-wide device state: tables on the device, default stream.
 struct Context {
@@ -180,7 +186,7 @@ inline int tc_bucket_mn(int m, int n) {
   return b < 5 ? b : 4;
 }
 
-constexpr int kTcFreqsPerCta = 16;  // = contract_tc_freqs() (frequencies per tensor-core CTA)
+constexpr int kTcFreqsPerCta = 128;  // = contract_tc_freqs() (frequencies per tensor-core CTA)
 
 Context& context();
 std::mutex& workspace_mutex();
@@ -290,7 +296,7 @@ class Plan {
   std::vector<ProdDesc> pd_;
   std::vector<ContractItem> items_;     // CUDA-core contraction work
   std::vector<ContractItem> tc_items_;  // tensor-core contraction work
-  int tc_max_m_ = 0, tc_max_k_ = 0, tc_max_n_ = 0;
+  std::vector<int> tc_shapes_;  // distinct (m, k, n) of the tensor-core products
   std::vector<Group> fwd_groups_, inv_groups_, rec_groups_;
   std::vector<uint32_t> idx_all_;
   std::vector<CtaItem> cta_items_;

@@ -1326,9 +1326,9 @@ __device__ __forceinline__ void load_freqs(const uint32_t* src, bool ok, int nf,
 }
 
 template <int F>
-__global__ void __launch_bounds__(tc::kThreads, 1)
+__global__ void __launch_bounds__(tc::kThreads, 2)
 k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
-              uint32_t* __restrict__ res, int tmem_cols, int* __restrict__ status, int stall) {
+              uint32_t* __restrict__ res, int bufcols, int* __restrict__ status, int stall) {
   extern __shared__ __align__(1024) uint8_t tsm[];
   __shared__ __align__(8) uint64_t bars[2];
   __shared__ uint32_t tmem_slot;
@@ -1345,13 +1345,18 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   const uint32_t mu = c_primes[j].mu;
   const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
   const tc::Shape sh = tc::shape_of(m, k, n);
-  const bool dbl = tc::double_buffered(sh);
+  const bool dbl = tc::double_buffered(bufcols);
+  const int tmem_cols = dbl ? 2 * bufcols : bufcols;
   const uint32_t ucols = (uint32_t)tc::unit_cols(sh);
+  // frequencies per unit: products with one column range put several
+  // frequencies' accumulators side by side in a TMEM buffer
+  const int gf = tc::group_freqs(sh, F, bufcols);
   const int plane_bytes = sh.m8 * sh.kp;
   uint8_t* As = tsm;
   uint8_t* Bs = As + F * sh.a_bytes;
   uint64_t* red = reinterpret_cast<uint64_t*>(Bs + F * sh.b_bytes);
-  uint32_t* outs = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(red) + sh.red_bytes);
+  uint32_t* outs =
+      reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(red) + gf * sh.red_bytes);
   const uint32_t a_base = tc::smem_u32(As), b_base = tc::smem_u32(Bs);
   const uint32_t barp[2] = {tc::smem_u32(&bars[0]), tc::smem_u32(&bars[1])};
 
@@ -1375,7 +1380,7 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   uint32_t phase[2] = {0u, 0u};
   int pending[2] = {0, 0};
   bool failed = false;
-  const int issue = stall ? 0 : 1;  // stall (failure-path tests only): no MMA, no commit
+  const int issue_mma = stall ? 0 : 1;  // stall (failure-path tests only): no MMA, no commit
 
   for (int fb0 = 0; fb0 < tc::kFreqs; fb0 += F) {
     const uint32_t hs = it.h0 + (uint32_t)fb0;
@@ -1385,49 +1390,70 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
 
     // ---- stage A' and B' of the nf frequencies: a warp task is 8 rows
     // (i of A, l of B) by 16 terms; a thread gathers four terms' residues
-    // of one row for every frequency and writes their byte planes
+    // of one row for every frequency and writes their byte planes.  Small F
+    // keeps TU tasks' loads in flight at once.
     const int kbn = sh.kp / 16;
     const int a_tasks = ((m + 7) / 8) * kbn;
     const int tasks = a_tasks + ((n + 7) / 8) * kbn;
-    for (int task = warp; task < tasks; task += tc::kThreads / 32) {
-      const bool isA = task < a_tasks;
-      const int tt = isA ? task : task - a_tasks;
-      const int rb = tt / kbn;
-      const int kb = tt - rb * kbn;
-      const int kk0 = 16 * kb + 4 * (lane & 3);
-      // A: lane -> (row i mod 8, term quad); B: lane -> (l mod 8, term quad)
-      const int r = 8 * rb + (isA ? ((lane >> 2) & 7) : (lane >> 2));
-      uint32_t x[4][F];
+    constexpr int TU = F <= 4 ? 2 : 1;
+    constexpr int kWarps = tc::kThreads / 32;
+    for (int task0 = warp; task0 < tasks; task0 += TU * kWarps) {
+      uint32_t x[TU][4][F];
+      int rr[TU], kq[TU];
+      bool isa[TU];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int kk = kk0 + c;
-        const bool ok = kk < k && r < (isA ? m : n);
-        const uint64_t poly = ok ? (isA ? (uint64_t)(r * k + kk) : (uint64_t)(kk * n + r)) : 0;
-        const uint32_t* src = res + (isA ? d.a_res : d.b_res) + poly * stride + base;
-        load_freqs<F>(src, ok, nf, x[c]);
+      for (int w2 = 0; w2 < TU; ++w2) {
+        const int task = task0 + w2 * kWarps;
+        const bool live = task < tasks;
+        const bool isA = task < a_tasks;
+        const int tt = isA ? task : task - a_tasks;
+        const int rb = tt / kbn;
+        const int kb = tt - rb * kbn;
+        const int kk0 = 16 * kb + 4 * (lane & 3);
+        // A: lane -> (row i mod 8, term quad); B: lane -> (l mod 8, term quad)
+        const int r = 8 * rb + (isA ? ((lane >> 2) & 7) : (lane >> 2));
+        rr[w2] = r;
+        kq[w2] = kk0;
+        isa[w2] = isA;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int kk = kk0 + c;
+          const bool ok = live && kk < k && r < (isA ? m : n);
+          const uint64_t poly =
+              ok ? (isA ? (uint64_t)(r * k + kk) : (uint64_t)(kk * n + r)) : 0;
+          const uint32_t* src = res + (isA ? d.a_res : d.b_res) + poly * stride + base;
+          load_freqs<F>(src, ok, nf, x[w2][c]);
+        }
       }
 #pragma unroll
-      for (int f = 0; f < F; ++f) {
-        if (f >= nf) break;
-        uint32_t pl[4];
-        tc::byte_planes(x[0][f], x[1][f], x[2][f], x[3][f], pl);
-        if (isA) {
-          // plane s of row i: rows s m8 + i; lanes cover (i mod 8, quad): no conflicts
-          uint8_t* t = As + f * sh.a_bytes + tc::tile_off((uint32_t)r, (uint32_t)kk0,
-                                                          (uint32_t)sh.kp);
+      for (int w2 = 0; w2 < TU; ++w2) {
+        if (task0 + w2 * kWarps >= tasks) break;  // uniform over the warp
+        const int r = rr[w2], kk0 = kq[w2];
 #pragma unroll
-          for (int s = 0; s < 4; ++s) *reinterpret_cast<uint32_t*>(t + s * plane_bytes) = pl[s];
-        } else {
-          // plane t of column l: row 4 l + t; the store order rotates with
-          // bits 3-4 of the lane so every store covers all 32 banks
-          uint8_t* t = Bs + f * sh.b_bytes;
-          const int g = (lane >> 3) & 3;
+        for (int f = 0; f < F; ++f) {
+          if (f >= nf) break;
+          uint32_t pl[4];
+          tc::byte_planes(x[w2][0][f], x[w2][1][f], x[w2][2][f], x[w2][3][f], pl);
+          if (isa[w2]) {
+            // plane s of row i: rows s m8 + i; lanes cover (i mod 8, quad): no conflicts
+            uint8_t* t = As + f * sh.a_bytes + tc::tile_off((uint32_t)r, (uint32_t)kk0,
+                                                            (uint32_t)sh.kp);
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int tp = (q + g) & 3;
-            const uint32_t v = tp == 0 ? pl[0] : (tp == 1 ? pl[1] : (tp == 2 ? pl[2] : pl[3]));
-            *reinterpret_cast<uint32_t*>(
-                t + tc::tile_off((uint32_t)(4 * r + tp), (uint32_t)kk0, (uint32_t)sh.kp)) = v;
+            for (int s2 = 0; s2 < 4; ++s2)
+              *reinterpret_cast<uint32_t*>(t + s2 * plane_bytes) = pl[s2];
+          } else {
+            // plane t of column l: row 4 l + t; the store order rotates with
+            // bits 3-4 of the lane so every store covers all 32 banks
+            uint8_t* t = Bs + f * sh.b_bytes;
+            const int g = (lane >> 3) & 3;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int tp = (q + g) & 3;
+              const uint32_t v =
+                  tp == 0 ? pl[0] : (tp == 1 ? pl[1] : (tp == 2 ? pl[2] : pl[3]));
+              *reinterpret_cast<uint32_t*>(
+                  t + tc::tile_off((uint32_t)(4 * r + tp), (uint32_t)kk0, (uint32_t)sh.kp)) = v;
+            }
           }
         }
       }
@@ -1435,22 +1461,42 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
-    // ---- units: MMAs, then the epilogue of each ----
-    const int U = nf * sh.nunits;
-    if (tid == 0 && issue) {
-      tc_issue_unit(sh, a_base, b_base, 0, tmem);
+    // ---- units: MMAs, then the epilogue of each.  A unit is gf
+    // frequencies (products with one column range) or one frequency's
+    // column range uu; its accumulators are consecutive in TMEM ----
+    const int U = sh.nunits == 1 ? (nf + gf - 1) / gf : nf * sh.nunits;
+    auto unit_freqs = [&](int u, int* f0, int* nfu, int* uu) {
+      if (sh.nunits == 1) {
+        *f0 = u * gf;
+        *nfu = (nf - *f0) < gf ? (nf - *f0) : gf;
+        *uu = 0;
+      } else {
+        *f0 = u / sh.nunits;
+        *nfu = 1;
+        *uu = u - *f0 * sh.nunits;
+      }
+    };
+    auto issue = [&](int u, uint32_t dcol) {
+      int f0, nfu, uu;
+      unit_freqs(u, &f0, &nfu, &uu);
+      for (int fi = 0; fi < nfu; ++fi)
+        tc_issue_unit(sh, a_base, b_base, (f0 + fi) * sh.nunits + uu,
+                      dcol + (uint32_t)fi * ucols);
+    };
+    if (tid == 0 && issue_mma) {
+      issue(0, tmem);
       tc_commit(barp[0]);
     }
-    pending[0] += issue;
+    pending[0] += issue_mma;
     for (int u = 0; u < U; ++u) {
       const int buf = dbl ? (u & 1) : 0;
       if (dbl && u + 1 < U) {  // the next unit's MMAs overlap this epilogue
         const int nb = (u + 1) & 1;
-        if (tid == 0 && issue) {
-          tc_issue_unit(sh, a_base, b_base, u + 1, tmem + (uint32_t)nb * ucols);
+        if (tid == 0 && issue_mma) {
+          issue(u + 1, tmem + (uint32_t)(nb * bufcols));
           tc_commit(barp[nb]);
         }
-        pending[nb] += issue;
+        pending[nb] += issue_mma;
       }
       const bool ok = tc::mbar_wait(barp[buf], phase[buf]);
       if (ok) {
@@ -1462,60 +1508,69 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int f = u / sh.nunits;
-      const int l0 = (u - f * sh.nunits) * sh.npl;
+      int f0, nfu, uu;
+      unit_freqs(u, &f0, &nfu, &uu);
+      const int l0 = uu * sh.npl;
       const int nl = (n - l0) < sh.npl ? (n - l0) : sh.npl;
       const int nch = (nl + 3) / 4;
       const int qd = warp & 3;
       const int lam = 32 * qd + lane;  // this thread's TMEM lane
       const int i = lam % sh.m8;       // its row (the same in every M tile)
-      const uint32_t laddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)buf * ucols;
-      for (int ch = warp >> 2; ch < nch; ch += 2) {  // warpgroups take alternate chunks
-        uint64_t part[4] = {0, 0, 0, 0};
-        for (int q = 0; q < sh.mt; ++q) {
-          uint32_t v[16];
-          tmem_ld16(laddr + (uint32_t)(q * sh.ncol + 16 * ch), v);
-          const int s = (128 * q + lam) / sh.m8;  // byte plane of this lane: warp-uniform
+      const uint32_t laddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(buf * bufcols);
+      for (int fi = 0; fi < nfu; ++fi) {
+        const int f = f0 + fi;
+        for (int ch = warp >> 2; ch < nch; ch += 2) {  // warpgroups take alternate chunks
+          uint64_t part[4] = {0, 0, 0, 0};
+          for (int q = 0; q < sh.mt; ++q) {
+            uint32_t v[16];
+            tmem_ld16(laddr + (uint32_t)(fi * (int)ucols + q * sh.ncol + 16 * ch), v);
+            const int s = (128 * q + lam) / sh.m8;  // byte plane of this lane: warp-uniform
 #pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const uint64_t w = c_primes[j].w8[s + t];
+            for (int t = 0; t < 4; ++t) {
+              const uint64_t w = c_primes[j].w8[s + t];
 #pragma unroll
-            for (int u2 = 0; u2 < 4; ++u2) part[u2] += (uint64_t)v[4 * u2 + t] * w;
+              for (int u2 = 0; u2 < 4; ++u2) part[u2] += (uint64_t)v[4 * u2 + t] * w;
+            }
           }
-        }
-        if (sh.g == 1) {  // all four planes of row i are in this lane
-          if (i < m) {
+          if (sh.g == 1) {  // all four planes of row i are in this lane
+            if (i < m) {
+#pragma unroll
+              for (int u2 = 0; u2 < 4; ++u2) {
+                const int l = 4 * ch + u2;
+                if (l < nl) outs[(i * n + l0 + l) * F + f] = redc64(part[u2], p, pinv, mu);
+              }
+            }
+          } else {
+            uint64_t* rf = red + fi * 128 * (sh.npl + 1);
 #pragma unroll
             for (int u2 = 0; u2 < 4; ++u2) {
               const int l = 4 * ch + u2;
-              if (l < nl) outs[(i * n + l0 + l) * F + f] = redc64(part[u2], p, pinv, mu);
+              if (l < nl) rf[lam * (sh.npl + 1) + l] = part[u2];
             }
-          }
-        } else {
-#pragma unroll
-          for (int u2 = 0; u2 < 4; ++u2) {
-            const int l = 4 * ch + u2;
-            if (l < nl) red[lam * (sh.npl + 1) + l] = part[u2];
           }
         }
       }
       if (sh.g > 1) {  // add the partial sums of the g lanes that hold row i
         __syncthreads();
-        for (int xo = tid; xo < m * nl; xo += tc::kThreads) {
-          const int ii = xo / nl, l = xo - ii * nl;
+        const int per = m * nl;
+        for (int xo = tid; xo < nfu * per; xo += tc::kThreads) {
+          const int fi = xo / per;
+          const int rem = xo - fi * per;
+          const int ii = rem / nl, l = rem - ii * nl;
+          const uint64_t* rf = red + fi * 128 * (sh.npl + 1);
           uint64_t z = 0;
-          for (int g2 = 0; g2 < sh.g; ++g2) z += red[(g2 * sh.m8 + ii) * (sh.npl + 1) + l];
-          outs[(ii * n + l0 + l) * F + f] = redc64(z, p, pinv, mu);
+          for (int g2 = 0; g2 < sh.g; ++g2) z += rf[(g2 * sh.m8 + ii) * (sh.npl + 1) + l];
+          outs[(ii * n + l0 + l) * F + f0 + fi] = redc64(z, p, pinv, mu);
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();
       if (!dbl && u + 1 < U) {
-        if (tid == 0 && issue) {
-          tc_issue_unit(sh, a_base, b_base, u + 1, tmem);
+        if (tid == 0 && issue_mma) {
+          issue(u + 1, tmem);
           tc_commit(barp[0]);
         }
-        pending[0] += issue;
+        pending[0] += issue_mma;
       }
     }
     if (failed) break;
@@ -1871,22 +1926,45 @@ bool contract_tc_eligible(int m, int k, int n) {
 // Frequencies staged at once (F), dynamic shared memory and TMEM columns of a
 // tensor-core launch whose products have at most max_m rows, max_k terms and
 // max_n columns: per-product layouts are all within these bounds.
-static bool tc_launch_config(int max_m, int max_k, int max_n, int* F, int* smem, int* tcols) {
-  const tc::Shape sh = tc::shape_of(max_m, max_k, max_n);
-  const int red = 128 * (sh.npl + 1) * 8;  // any product with fewer rows may need it
-  const int budget = tc::kDynSmemLimit;
-  for (int f = 16; f >= 1; f >>= 1) {
-    const int out = ((max_m * max_n * f * 4) + 15) & ~15;
-    const int bytes = f * (sh.a_bytes + sh.b_bytes) + red + out;
-    if (bytes <= budget) {
-      *F = f;
-      *smem = bytes;
-      const int uc = tc::unit_cols(sh);
-      int need = 2 * uc <= 512 ? 2 * uc : 512;
-      int c = 32;
-      while (c < need) c <<= 1;
-      *tcols = c;
-      return true;
+// Dynamic shared memory of one product's CTA with F frequencies staged:
+// byte tiles, the lane-sum buffer of a unit, the results of the F frequencies.
+int tc_smem_bytes(int m, int k, int n, int F, int bufcols) {
+  const tc::Shape sh = tc::shape_of(m, k, n);
+  const int out = ((m * n * F * 4) + 15) & ~15;
+  return F * (sh.a_bytes + sh.b_bytes) + tc::group_freqs(sh, F, bufcols) * sh.red_bytes + out;
+}
+
+// Accumulator buffer width, frequencies staged at once (F) and dynamic shared
+// memory of a launch over products of the given shapes.  The buffer is the
+// widest accumulator rounded up to a power of two (narrow products then
+// leave TMEM for a second CTA on the SM); F is the largest that lets as many
+// CTAs share an SM as TMEM allows (at most two), else the largest that fits.
+static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* F, int* smem) {
+  int widest = 0;
+  for (int i = 0; i < nshapes; ++i) {
+    const int c = tc::unit_cols(tc::shape_of(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]));
+    if (c > widest) widest = c;
+  }
+  int b = 32;
+  while (b < widest) b <<= 1;
+  *bufcols = b;
+  const int tcols = tc::double_buffered(b) ? 2 * b : b;
+  const int per_sm = 512 / tcols >= 2 ? 2 : 1;
+  for (int target = per_sm; target >= 1; --target) {
+    const int limit = target == 1 ? tc::kDynSmemLimit
+                                  : (tc::kSmemLimit / target) - tc::kStaticSmem - 1024;
+    for (int f = 16; f >= 1; f >>= 1) {
+      int bytes = 0;
+      for (int i = 0; i < nshapes; ++i) {
+        const int sb = tc_smem_bytes(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], f, b);
+        if (sb > bytes) bytes = sb;
+      }
+      // below four staged frequencies a second CTA is not worth the loss
+      if (bytes <= limit && (target == 1 || f >= 4)) {
+        *F = f;
+        *smem = bytes;
+        return true;
+      }
     }
   }
   return false;
@@ -1894,24 +1972,27 @@ static bool tc_launch_config(int max_m, int max_k, int max_n, int* F, int* smem,
 
 template <int F>
 static void launch_tc_f(int count, int smem, cudaStream_t st, const ProdDesc* prods,
-                        const ContractItem* items, uint32_t* res, int tcols, int* status,
+                        const ContractItem* items, uint32_t* res, int bufcols, int* status,
                         int stall) {
-  k_contract_tc<F><<<count, tc::kThreads, smem, st>>>(prods, items, res, tcols, status, stall);
+  k_contract_tc<F><<<count, tc::kThreads, smem, st>>>(prods, items, res, bufcols, status,
+                                                      stall);
 }
 
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
-                               uint32_t* res, int max_m, int max_k, int max_n, int* status,
+                               uint32_t* res, const int* shapes, int nshapes, int* status,
                                cudaStream_t st, int stall) {
   if (count == 0) return cudaSuccess;
-  if (!contract_tc_eligible(max_m, max_k, max_n)) return cudaErrorInvalidValue;
-  int F = 0, smem = 0, tcols = 0;
-  if (!tc_launch_config(max_m, max_k, max_n, &F, &smem, &tcols)) return cudaErrorInvalidValue;
+  for (int i = 0; i < nshapes; ++i)
+    if (!contract_tc_eligible(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]))
+      return cudaErrorInvalidValue;
+  int F = 0, smem = 0, bufcols = 0;
+  if (!tc_launch_config(shapes, nshapes, &bufcols, &F, &smem)) return cudaErrorInvalidValue;
   switch (F) {
-    case 16: launch_tc_f<16>(count, smem, st, prods, items, res, tcols, status, stall); break;
-    case 8: launch_tc_f<8>(count, smem, st, prods, items, res, tcols, status, stall); break;
-    case 4: launch_tc_f<4>(count, smem, st, prods, items, res, tcols, status, stall); break;
-    case 2: launch_tc_f<2>(count, smem, st, prods, items, res, tcols, status, stall); break;
-    default: launch_tc_f<1>(count, smem, st, prods, items, res, tcols, status, stall); break;
+    case 16: launch_tc_f<16>(count, smem, st, prods, items, res, bufcols, status, stall); break;
+    case 8: launch_tc_f<8>(count, smem, st, prods, items, res, bufcols, status, stall); break;
+    case 4: launch_tc_f<4>(count, smem, st, prods, items, res, bufcols, status, stall); break;
+    case 2: launch_tc_f<2>(count, smem, st, prods, items, res, bufcols, status, stall); break;
+    default: launch_tc_f<1>(count, smem, st, prods, items, res, bufcols, status, stall); break;
   }
   return cudaGetLastError();
 }

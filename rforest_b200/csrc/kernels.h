@@ -61,14 +61,16 @@ cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_
                               cudaStream_t st);
 
 // Tensor-core contraction (tcgen05 kind::i8) for products with m <= 128,
-// k <= 64, n <= 64 (max_m, max_k, max_n: the launch's largest); each work
-// item covers contract_tc_freqs() consecutive frequencies.  *status is set
-// to 1 if a bounded wait gave up.  stall != 0 (failure-path tests only)
-// issues no tensor work, so every CTA's wait runs out.
+// k <= 64, n <= 64; shapes: the launch's distinct (m, k, n), nshapes triples
+// (they size its shared memory); each work item covers contract_tc_freqs()
+// consecutive frequencies.  *status is set to 1 if a bounded wait gave up.
+// stall != 0 (failure-path tests only) issues no tensor work, so every CTA's
+// wait runs out.
 bool contract_tc_eligible(int m, int k, int n);
 int contract_tc_freqs();
+int tc_smem_bytes(int m, int k, int n, int F, int bufcols);
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
-                               uint32_t* res, int max_m, int max_k, int max_n, int* status,
+                               uint32_t* res, const int* shapes, int nshapes, int* status,
                                cudaStream_t st, int stall = 0);
 
 // CRT + recompose + sign for `count` output entries with P primes; rmin is

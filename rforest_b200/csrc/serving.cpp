@@ -38,6 +38,7 @@ struct Ticket {
   uint64_t id = 0;
   ProductSpec spec;
   int64_t bytes = 0;
+  int64_t host_bytes = 0;  // inputs + outputs across the link
   int64_t t_submit = 0, t_start = 0, t_done = 0;
   int status = -1;  // -1 pending
   std::string error;
@@ -59,6 +60,10 @@ struct mpzmm_server {
   // admission window: a slot that frees up while other batches occupy the
   // GPU keeps admitting for up to this long before it launches (ns)
   int64_t window_ns = 200000;
+  // host bytes (inputs + outputs) of a batch: admission stops there (a
+  // larger request goes alone), and every slot's pinned staging is sized to
+  // it once, so batches never allocate pinned memory
+  int64_t batch_host_cap = (int64_t)256 << 20;
   // device memory of the slots' workspaces: a stream-ordered pool of the
   // server's own that keeps freed memory, so a workspace growing or being
   // released never synchronises the device or stalls the other slots
@@ -90,13 +95,17 @@ struct mpzmm_server {
   void admit(std::vector<std::shared_ptr<Ticket>>& batch, int64_t& bytes) {
     int busy_slots = 0;
     for (auto& o : slots) busy_slots += o->busy ? 1 : 0;
+    int64_t host = 0;
+    for (const auto& t : batch) host += t->host_bytes;
     while (!queue.empty() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
       const auto& t = queue.front();
+      if (!batch.empty() && host + t->host_bytes > batch_host_cap) break;
       const bool fits = in_flight_bytes + bytes + t->bytes <= budget;
       const bool alone = batch.empty() && busy_slots == 0 && in_flight_bytes == 0 &&
                          t->bytes <= budget;
       if (!fits && !alone) break;
       bytes += t->bytes;
+      host += t->host_bytes;
       batch.push_back(t);
       queue.pop_front();
       if (!fits) break;
@@ -136,6 +145,10 @@ struct mpzmm_server {
 
   void slot_loop(Slot& s) {
     cudaSetDevice(device);
+    // pinned staging for a full batch, once (a failure here only means the
+    // first batches grow it instead)
+    if (s.ws.reserve_staging((size_t)(batch_host_cap / 8), (size_t)(batch_host_cap / 4)))
+      cudaGetLastError();
     for (;;) {
       std::vector<std::shared_ptr<Ticket>> batch;
       int64_t bytes = 0;
@@ -263,7 +276,7 @@ int mpzmm_server_submit(mpzmm_server* s, const mpzmm_product* req, uint64_t* tic
     t->spec.b[e] = EntryRef{p.b_sizes[e] ? p.b_limbs + p.b_offs[e] : nullptr, p.b_sizes[e]};
   for (int64_t e = 0; e < nc; ++e)
     t->spec.c[e] = OutRef{p.c_limbs + p.c_offs[e], p.c_caps[e], p.c_sizes + e, nullptr};
-  t->bytes = estimate_device_bytes(t->spec);
+  t->bytes = estimate_device_bytes(t->spec, &t->host_bytes);
   if (t->bytes < 0) return set_error(kErrTooLarge, "product too large for a single transform");
   if (t->bytes > s->budget)
     return set_error(kErrTooLarge, "request needs " + std::to_string(t->bytes) +
