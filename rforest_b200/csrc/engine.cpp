@@ -600,6 +600,13 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.c_res = n_res_;
     n_res_ += (uint64_t)m * n * poly;
+    // contraction engine: tensor cores where the mode or the autotuner says
+    // so, for transforms of 8 .. 2^15 points (their operands are written in
+    // the frequency-blocked layout by the one-CTA forward kernels)
+    const int mode = context().contract_mode;
+    const bool use_tc = contract_tc_eligible(m, k, n) && lgN >= 3 && lgN <= kMaxLgNOneCta &&
+                        (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)]
+                                                                     [tc_bucket_mn(m, n)] == 1));
     Group& fg = fwdg[{lgN, P * 16 + (r + 29) / 30}];  // one class per product
     fg.P = P;
     fg.lgN = lgN;
@@ -626,6 +633,11 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
           fd.lgN = (uint16_t)lgN;
           fd.P = (uint16_t)P;
           fd.ncoef = (uint32_t)N;  // replaced on the device
+          if (use_tc) {  // the operand block, entry e of it
+            fd.res_off = base;
+            fd.tile_np = (uint32_t)ents.size();
+            fd.tile_e = (uint32_t)e;
+          }
           fg.idx.push_back((uint32_t)fwd_.size());
           fwd_.push_back(fd);
         }
@@ -665,6 +677,11 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
         fd.limb_off = n_limbs_;
         n_limbs_ += (uint64_t)nl;
         fd.res_off = base + e * poly;
+        if (use_tc) {  // the operand block, entry e of it (frequency-blocked layout)
+          fd.res_off = base;
+          fd.tile_np = (uint32_t)ents.size();
+          fd.tile_e = (uint32_t)e;
+        }
         fd.size = ents[e].size;
         fd.r = (uint32_t)r;
         fd.lgN = (uint16_t)lgN;
@@ -677,9 +694,6 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     }
     const uint32_t prod_index = (uint32_t)pd_.size();
     pd_.push_back(pd);
-    const int mode = context().contract_mode;
-    const bool use_tc = contract_tc_eligible(m, k, n) &&
-                        (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)][tc_bucket_mn(m, n)] == 1));
     if (use_tc) {
       bool seen = false;
       for (size_t q = 0; q < tc_shapes_.size() && !seen; q += 3)
@@ -796,13 +810,19 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
     }
     if (g.idx.empty()) continue;
     g.crt_high = high != 0;
-    // longest entries first (the warp that gets one works longest), ties in
-    // entry order: one sort of packed (longest-first key, index) integers
+    // entries grouped by prime count (warps running at the same time then
+    // share one unrolled variant, which keeps the instruction cache warm),
+    // longest first within a count (the warp that gets one works longest),
+    // ties in entry order: one sort of packed (count, length, index) keys --
+    // out_words < 2^26 (bit positions are 31-bit) and indices < 2^31
     std::vector<uint64_t> keys(g.idx.size());
-    for (size_t i = 0; i < keys.size(); ++i)
-      keys[i] = ((uint64_t)(0xffffffffu - inv_[g.idx[i]].out_words) << 32) | g.idx[i];
+    for (size_t i = 0; i < keys.size(); ++i) {
+      const InvDesc& d = inv_[g.idx[i]];
+      keys[i] = ((uint64_t)(kMaxPrimes - d.P) << 57) |
+                ((uint64_t)((1u << 26) - 1u - d.out_words) << 31) | g.idx[i];
+    }
     std::sort(keys.begin(), keys.end());
-    for (size_t i = 0; i < keys.size(); ++i) g.idx[i] = (uint32_t)keys[i];
+    for (size_t i = 0; i < keys.size(); ++i) g.idx[i] = (uint32_t)(keys[i] & 0x7fffffffu);
     rec_groups_.push_back(std::move(g));
   }
   for (auto* gs : {&fwd_groups_, &inv_groups_, &rec_groups_})

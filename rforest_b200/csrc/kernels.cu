@@ -400,9 +400,27 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
   return neg ? 3u * p - v : v;
 }
 
-// 2^L consecutive points reduced from [0, 4p) to [0, p), vector stores
+// Where the forward transform leaves point h of prime j of an entry: the
+// plain frequency-contiguous layout (base + j N + h), or, for an operand of a
+// tensor-core product, blocked by kTcTile frequencies across the operand's
+// np entries (base + ((j N / 4 + h / 4) np + e) 4 + h mod 4).
+struct FwdOut {
+  uint32_t* base;
+  uint32_t np, e;
+  int lgN;
+  __device__ __forceinline__ uint32_t* at(int j, uint32_t h) const {
+    if (np == 0) return base + ((uint64_t)j << lgN) + h;
+    const uint64_t tile = ((uint64_t)j << (lgN - 2)) + (h >> 2);
+    return base + (tile * np + e) * (uint64_t)kTcTile + (h & 3u);
+  }
+};
+
+// 2^L consecutive points h0 .. (h0 a multiple of 2^L) reduced from [0, 4p)
+// to [0, p), vector stores (a 4-point run never crosses a block)
 template <int L>
-__device__ __forceinline__ void store_points(uint32_t* dst, uint32_t* a, uint32_t p) {
+__device__ __forceinline__ void store_points(const FwdOut& fo, int j, uint32_t h0, uint32_t* a,
+                                             uint32_t p) {
+  static_assert(kTcTile == 4, "vector stores assume 4-frequency blocks");
   const uint32_t p2 = 2 * p;
 #pragma unroll
   for (int q = 0; q < (1 << L); ++q) {
@@ -410,25 +428,25 @@ __device__ __forceinline__ void store_points(uint32_t* dst, uint32_t* a, uint32_
     a[q] = v >= p ? v - p : v;
   }
   if (L == 3) {
-    reinterpret_cast<uint4*>(dst)[0] = make_uint4(a[0], a[1], a[2], a[3]);
-    reinterpret_cast<uint4*>(dst)[1] = make_uint4(a[4], a[5], a[6], a[7]);
+    *reinterpret_cast<uint4*>(fo.at(j, h0)) = make_uint4(a[0], a[1], a[2], a[3]);
+    *reinterpret_cast<uint4*>(fo.at(j, h0 + 4)) = make_uint4(a[4], a[5], a[6], a[7]);
   } else if (L == 2) {
-    reinterpret_cast<uint4*>(dst)[0] = make_uint4(a[0], a[1], a[2], a[3]);
+    *reinterpret_cast<uint4*>(fo.at(j, h0)) = make_uint4(a[0], a[1], a[2], a[3]);
   } else {
-    reinterpret_cast<uint2*>(dst)[0] = make_uint2(a[0], a[1]);
+    *reinterpret_cast<uint2*>(fo.at(j, h0)) = make_uint2(a[0], a[1]);
   }
 }
 
 template <int LP>
-__device__ __forceinline__ void fwd_last_pass(const uint32_t* s, uint32_t* out, bool valid,
-                                              int lgN, int last_s0, int tt, int TS,
+__device__ __forceinline__ void fwd_last_pass(const uint32_t* s, const FwdOut& fo, int j,
+                                              bool valid, int lgN, int last_s0, int tt, int TS,
                                               const uint2* __restrict__ tw, uint32_t p) {
   for (int g = tt; g < ((1 << lgN) >> LP); g += TS) {
     uint32_t a[1 << LP];
 #pragma unroll
     for (int q = 0; q < (1 << LP); ++q) a[q] = s[smi((g << LP) + q)];
     fwd_group<LP>(a, last_s0, g, tw, p);
-    if (valid) store_points<LP>(out + (g << LP), a, p);
+    if (valid) store_points<LP>(fo, j, (uint32_t)(g << LP), a, p);
   }
 }
 
@@ -470,10 +488,14 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
     }
     __syncthreads();
   }
+  FwdOut fo;
+  fo.base = res + d.res_off;
+  fo.np = d.tile_np;
+  fo.e = d.tile_e;
+  fo.lgN = lgN;
   for (int j = 0; j < P; ++j) {
     const uint32_t p = c_primes[j].p;
     const uint2* tw = twf + (size_t)j * kTwStride;
-    uint32_t* out = res + d.res_off + (uint64_t)j * (uint64_t)N;
     for (int g = tt; g < ng0; g += TS) {
       uint32_t a[8];
 #pragma unroll
@@ -496,7 +518,7 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
         fwd_group<3>(a, 0, 0, tw, p);
       }
       if (lgN == 3) {  // the only pass: eight consecutive points, straight out
-        if (valid) store_points<3>(out, a, p);
+        if (valid) store_points<3>(fo, j, 0u, a, p);
       } else {
 #pragma unroll
         for (int q = 0; q < 8; ++q) s[smi(q * ng0 + g)] = a[q];
@@ -512,9 +534,9 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
     // the last pass works on groups of 2^LP consecutive points: reduced and
     // stored straight from registers with vector stores
     switch (lgN - last_s0) {
-      case 1: fwd_last_pass<1>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
-      case 2: fwd_last_pass<2>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
-      default: fwd_last_pass<3>(s, out, valid, lgN, last_s0, tt, TS, tw, p); break;
+      case 1: fwd_last_pass<1>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
+      case 2: fwd_last_pass<2>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
+      default: fwd_last_pass<3>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
     }
     __syncthreads();  // before the next prime's first pass overwrites s
   }
@@ -919,7 +941,13 @@ k_ntt_blocks(const FwdDesc* __restrict__ fdescs, const InvDesc* __restrict__ ide
         smem_pass<3, true>(sm, lgC, s0, 3, tid, kFwdThreads, tw, p);
         __syncthreads();
       }
-      fwd_last_pass<3>(sm, io, true, lgC, last_s0, tid, kFwdThreads, tw, p);
+      // a four-step block: plain layout, the block's points from b C on
+      FwdOut fo;
+      fo.base = res + off + ((uint64_t)b << lgC);
+      fo.np = 0;
+      fo.e = 0;
+      fo.lgN = lgN;
+      fwd_last_pass<3>(sm, fo, j, true, lgC, last_s0, tid, kFwdThreads, tw, p);
       __syncthreads();
     } else {
       for (int g = tid; g < C / 8; g += kFwdThreads) {
@@ -1305,15 +1333,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// F consecutive residues (frequencies hs .. hs + F - 1) of one polynomial;
-// only nf of them exist when the transform is shorter than the block
+// F consecutive residues (frequencies hs .. hs + F - 1) of entry e of an
+// operand stored in the blocked layout (FwdOut): blk is the operand block, np
+// its entries, tile the block of frequency hs (prime j included: j N/4 +
+// hs/4).  Only nf of them exist when the transform is shorter than the
+// CTA's frequencies.  Lanes take consecutive entries, so a warp's loads are
+// one contiguous run per 4 frequencies.
 template <int F>
-__device__ __forceinline__ void load_freqs(const uint32_t* src, bool ok, int nf,
-                                           uint32_t (&x)[F]) {
-  if (ok && nf == F && F >= 4) {
+__device__ __forceinline__ void load_freqs(const uint32_t* __restrict__ blk, uint64_t np,
+                                           uint64_t e, uint64_t tile, uint32_t sub, bool ok,
+                                           int nf, uint32_t (&x)[F]) {
+  if (ok && nf == F && F >= 4) {  // sub == 0: F / 4 whole blocks
 #pragma unroll
     for (int c = 0; c < F / 4; ++c) {
-      const uint4 u = __ldg(reinterpret_cast<const uint4*>(src) + c);
+      const uint4 u = __ldg(reinterpret_cast<const uint4*>(blk + ((tile + c) * np + e) * 4));
       x[4 * c] = u.x;
       x[4 * c + 1] = u.y;
       x[4 * c + 2] = u.z;
@@ -1321,7 +1354,10 @@ __device__ __forceinline__ void load_freqs(const uint32_t* src, bool ok, int nf,
     }
   } else {
 #pragma unroll
-    for (int f = 0; f < F; ++f) x[f] = (ok && f < nf) ? __ldg(src + f) : 0u;
+    for (int f = 0; f < F; ++f) {
+      const uint32_t h = sub + (uint32_t)f;
+      x[f] = (ok && f < nf) ? __ldg(blk + ((tile + (h >> 2)) * np + e) * 4 + (h & 3u)) : 0u;
+    }
   }
 }
 
@@ -1387,6 +1423,9 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     if (hs >= (uint32_t)N) break;  // uniform over the CTA
     const int nf = (int)((uint32_t)N - hs < (uint32_t)F ? (uint32_t)N - hs : (uint32_t)F);
     const uint64_t base = (uint64_t)j * (uint64_t)N + hs;
+    // the operands' blocked layout: frequency block of hs, offset inside it
+    const uint64_t tile0 = ((uint64_t)j << (d.lgN - 2)) + (hs >> 2);
+    const uint32_t sub0 = hs & 3u;
 
     // ---- stage A' and B' of the nf frequencies: a warp task is 8 rows
     // (i of A, l of B) by 16 terms; a thread gathers four terms' residues
@@ -1421,8 +1460,8 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
           const bool ok = live && kk < k && r < (isA ? m : n);
           const uint64_t poly =
               ok ? (isA ? (uint64_t)(r * k + kk) : (uint64_t)(kk * n + r)) : 0;
-          const uint32_t* src = res + (isA ? d.a_res : d.b_res) + poly * stride + base;
-          load_freqs<F>(src, ok, nf, x[w2][c]);
+          load_freqs<F>(res + (isA ? d.a_res : d.b_res), isA ? (uint64_t)m * k : (uint64_t)k * n,
+                        poly, tile0, sub0, ok, nf, x[w2][c]);
         }
       }
 #pragma unroll

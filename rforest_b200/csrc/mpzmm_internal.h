@@ -81,7 +81,14 @@ struct FwdDesc {
   uint16_t lgN;
   uint16_t P;
   uint32_t ncoef;      // coefficients to split (<= N)
+  // Operand of a tensor-core product: its residues are blocked by
+  // kTcTile frequencies across the operand's tile_np entries (res_off is the
+  // operand block, tile_e this entry), so one frequency block of every entry
+  // is one contiguous run; tile_np == 0: the plain layout above.
+  uint32_t tile_np = 0;
+  uint32_t tile_e = 0;
 };
+constexpr int kTcTile = 4;  // frequencies a block of the tensor-core layout
 
 // One output polynomial of the inverse transform + CRT + recompose.
 struct InvDesc {

@@ -193,6 +193,8 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
     f.P = (uint16_t)P;
     const uint64_t nco = ((uint64_t)nl * 64 + r - 1) / r;
     f.ncoef = (uint32_t)(nco < N ? nco : N);
+    f.tile_np = 0;  // plain layout (this entry point contracts on CUDA cores)
+    f.tile_e = 0;
     idx[i] = (uint32_t)i;
   }
   int64_t it = 0;
