@@ -17,7 +17,8 @@
 // Montgomery-reduces it, so C carries the same 2^-32 factor as the CUDA-core
 // contraction.
 //
-// One CTA of 256 threads per (product, prime, block of 128 frequencies),
+// One CTA of 256 threads (512 where it has the SM to itself) per (product,
+// prime, block of 128 frequencies),
 // processed F frequencies at a time: all warps stage A' and B' of the F
 // frequencies straight from global memory (F consecutive residues of a
 // polynomial per vector load) into canonical K-major no-swizzle tiles (8-row
@@ -26,8 +27,8 @@
 // product with at most 32 output columns, else one frequency's 32 columns),
 // tcgen05.commit arrives on the unit's mbarrier; with two 256-column TMEM
 // buffers the next unit's MMAs run while all eight warps drain the
-// current one (warp w reads TMEM lanes 32 (w mod 4) .. + 31, the two
-// warpgroups take alternate 16-column chunks).  Results of the F
+// current one (warp w reads TMEM lanes 32 (w mod 4) .. + 31, the
+// warpgroups take turns at 16-column chunks).  Results of the F
 // frequencies are gathered in shared memory and stored F residues per vector
 // store.  Every wait is bounded (one second of wall time): on time-out the
 // CTA records an error, waits (bounded) for MMAs it has issued, frees its
@@ -39,7 +40,7 @@
 namespace mpzmm {
 namespace tc {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;    // threads of a CTA that shares its SM (512 alone)
 constexpr int kMaxK = 64;        // k <= 64: K' = k bytes padded to 32, z < 2^57
 constexpr int kMaxN = 64;        // n <= 64: at most two units of 32 outputs a frequency
 constexpr int kMaxM = 128;       // m <= 128: four planes in four 128-lane tiles

@@ -279,6 +279,7 @@ class Plan {
     bool batched = false;
     bool team = false;
     bool large = false;    // four-step transform (2^lgN above one CTA)
+    bool tiled = false;    // forward: operands of tensor-core products (blocked layout)
     int D = 0;
     int max_lgN = 0;
     std::vector<CtaItem> items;

@@ -404,12 +404,15 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
 // plain frequency-contiguous layout (base + j N + h), or, for an operand of a
 // tensor-core product, blocked by kTcTile frequencies across the operand's
 // np entries (base + ((j N / 4 + h / 4) np + e) 4 + h mod 4).
+// TILED is a template flag so that plain launches carry none of the
+// blocked layout's state.
+template <bool TILED>
 struct FwdOut {
   uint32_t* base;
   uint32_t np, e;
   int lgN;
   __device__ __forceinline__ uint32_t* at(int j, uint32_t h) const {
-    if (np == 0) return base + ((uint64_t)j << lgN) + h;
+    if (!TILED) return base + ((uint64_t)j << lgN) + h;
     const uint64_t tile = ((uint64_t)j << (lgN - 2)) + (h >> 2);
     return base + (tile * np + e) * (uint64_t)kTcTile + (h & 3u);
   }
@@ -417,9 +420,9 @@ struct FwdOut {
 
 // 2^L consecutive points h0 .. (h0 a multiple of 2^L) reduced from [0, 4p)
 // to [0, p), vector stores (a 4-point run never crosses a block)
-template <int L>
-__device__ __forceinline__ void store_points(const FwdOut& fo, int j, uint32_t h0, uint32_t* a,
-                                             uint32_t p) {
+template <int L, bool TILED>
+__device__ __forceinline__ void store_points(const FwdOut<TILED>& fo, int j, uint32_t h0,
+                                             uint32_t* a, uint32_t p) {
   static_assert(kTcTile == 4, "vector stores assume 4-frequency blocks");
   const uint32_t p2 = 2 * p;
 #pragma unroll
@@ -437,8 +440,8 @@ __device__ __forceinline__ void store_points(const FwdOut& fo, int j, uint32_t h
   }
 }
 
-template <int LP>
-__device__ __forceinline__ void fwd_last_pass(const uint32_t* s, const FwdOut& fo, int j,
+template <int LP, bool TILED>
+__device__ __forceinline__ void fwd_last_pass(const uint32_t* s, const FwdOut<TILED>& fo, int j,
                                               bool valid, int lgN, int last_s0, int tt, int TS,
                                               const uint2* __restrict__ tw, uint32_t p) {
   for (int g = tt; g < ((1 << lgN) >> LP); g += TS) {
@@ -446,7 +449,7 @@ __device__ __forceinline__ void fwd_last_pass(const uint32_t* s, const FwdOut& f
 #pragma unroll
     for (int q = 0; q < (1 << LP); ++q) a[q] = s[smi((g << LP) + q)];
     fwd_group<LP>(a, last_s0, g, tw, p);
-    if (valid) store_points<LP>(fo, j, (uint32_t)(g << LP), a, p);
+    if (valid) store_points<LP, TILED>(fo, j, (uint32_t)(g << LP), a, p);
   }
 }
 
@@ -456,7 +459,7 @@ __device__ __forceinline__ void fwd_last_pass(const uint32_t* s, const FwdOut& f
 // and residues are skipped and stage 0 only copies.  dig (whole-CTA HZ
 // transforms, NULL otherwise): shared memory for the entry's digits, digit q
 // of coefficient x at dig[q N/2 + x], extracted once for all P primes.
-template <int D, bool TEAM, bool HZ>
+template <int D, bool TEAM, bool HZ, bool TILED>
 __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t* dig,
                                          bool valid, int lgN, int P, int tt, int TS,
                                          const uint64_t* __restrict__ limbs,
@@ -488,7 +491,7 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
     }
     __syncthreads();
   }
-  FwdOut fo;
+  FwdOut<TILED> fo;
   fo.base = res + d.res_off;
   fo.np = d.tile_np;
   fo.e = d.tile_e;
@@ -518,7 +521,7 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
         fwd_group<3>(a, 0, 0, tw, p);
       }
       if (lgN == 3) {  // the only pass: eight consecutive points, straight out
-        if (valid) store_points<3>(fo, j, 0u, a, p);
+        if (valid) store_points<3, TILED>(fo, j, 0u, a, p);
       } else {
 #pragma unroll
         for (int q = 0; q < 8; ++q) s[smi(q * ng0 + g)] = a[q];
@@ -534,9 +537,9 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
     // the last pass works on groups of 2^LP consecutive points: reduced and
     // stored straight from registers with vector stores
     switch (lgN - last_s0) {
-      case 1: fwd_last_pass<1>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
-      case 2: fwd_last_pass<2>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
-      default: fwd_last_pass<3>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
+      case 1: fwd_last_pass<1, TILED>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
+      case 2: fwd_last_pass<2, TILED>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
+      default: fwd_last_pass<3, TILED>(s, fo, j, valid, lgN, last_s0, tt, TS, tw, p); break;
     }
     __syncthreads();  // before the next prime's first pass overwrites s
   }
@@ -545,7 +548,7 @@ __device__ __forceinline__ void fwd_body(const FwdDesc& d, uint32_t* s, uint32_t
 // dig_words: shared memory words after the transform reserved for the digit
 // cache of a whole-CTA launch (0: none); it holds D N/2 words for the CTA's
 // transform size.
-template <int D, bool TEAM>
+template <int D, bool TEAM, bool TILED>
 __global__ void __launch_bounds__(kFwdThreads, 3)
 k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
        const CtaItem* __restrict__ items, const uint64_t* __restrict__ limbs,
@@ -570,9 +573,9 @@ k_fwd2(const FwdDesc* __restrict__ descs, const uint32_t* __restrict__ idx,
   if (valid) d = descs[idx[item.first + team]];
   // one variant for the whole CTA (its barriers must be the same code)
   if (__syncthreads_and(d.ncoef <= (uint32_t)(N >> 1)))
-    fwd_body<D, TEAM, true>(d, s, dig, valid, lgN, P, tt, TS, limbs, res, twf);
+    fwd_body<D, TEAM, true, TILED>(d, s, dig, valid, lgN, P, tt, TS, limbs, res, twf);
   else
-    fwd_body<D, TEAM, false>(d, s, nullptr, valid, lgN, P, tt, TS, limbs, res, twf);
+    fwd_body<D, TEAM, false, TILED>(d, s, nullptr, valid, lgN, P, tt, TS, limbs, res, twf);
 }
 
 // Inverse NTT, register-blocked (lgN >= 3): the forward passes backwards.
@@ -942,7 +945,7 @@ k_ntt_blocks(const FwdDesc* __restrict__ fdescs, const InvDesc* __restrict__ ide
         __syncthreads();
       }
       // a four-step block: plain layout, the block's points from b C on
-      FwdOut fo;
+      FwdOut<false> fo;
       fo.base = res + off + ((uint64_t)b << lgC);
       fo.np = 0;
       fo.e = 0;
@@ -1361,8 +1364,10 @@ __device__ __forceinline__ void load_freqs(const uint32_t* __restrict__ blk, uin
   }
 }
 
-template <int F>
-__global__ void __launch_bounds__(tc::kThreads, 2)
+// NT threads: 256 where two CTAs share an SM, 512 where one CTA has it to
+// itself (more warps to cover the staging and epilogue latency).
+template <int F, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
               uint32_t* __restrict__ res, int bufcols, int* __restrict__ status, int stall) {
   extern __shared__ __align__(1024) uint8_t tsm[];
@@ -1435,7 +1440,7 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     const int a_tasks = ((m + 7) / 8) * kbn;
     const int tasks = a_tasks + ((n + 7) / 8) * kbn;
     constexpr int TU = F <= 4 ? 2 : 1;
-    constexpr int kWarps = tc::kThreads / 32;
+    constexpr int kWarps = NT / 32;
     for (int task0 = warp; task0 < tasks; task0 += TU * kWarps) {
       uint32_t x[TU][4][F];
       int rr[TU], kq[TU];
@@ -1558,7 +1563,7 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
       const uint32_t laddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(buf * bufcols);
       for (int fi = 0; fi < nfu; ++fi) {
         const int f = f0 + fi;
-        for (int ch = warp >> 2; ch < nch; ch += 2) {  // warpgroups take alternate chunks
+        for (int ch = warp >> 2; ch < nch; ch += NT / 128) {  // warpgroups share the chunks
           uint64_t part[4] = {0, 0, 0, 0};
           for (int q = 0; q < sh.mt; ++q) {
             uint32_t v[16];
@@ -1592,7 +1597,7 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
       if (sh.g > 1) {  // add the partial sums of the g lanes that hold row i
         __syncthreads();
         const int per = m * nl;
-        for (int xo = tid; xo < nfu * per; xo += tc::kThreads) {
+        for (int xo = tid; xo < nfu * per; xo += NT) {
           const int fi = xo / per;
           const int rem = xo - fi * per;
           const int ii = rem / nl, l = rem - ii * nl;
@@ -1614,7 +1619,7 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     }
     if (failed) break;
     // ---- the nf frequencies of every output, F residues a vector store ----
-    for (int e = tid; e < m * n; e += tc::kThreads) {
+    for (int e = tid; e < m * n; e += NT) {
       uint32_t* dst = res + d.c_res + (uint64_t)e * stride + base;
       const uint32_t* sv = outs + e * F;
       if (nf == F && F >= 4) {
@@ -1816,7 +1821,7 @@ static int ntt_threads(int lgN) {
   return half < 32 ? 32 : (half > 1024 ? 1024 : half);
 }
 
-template <int D>
+template <int D, bool TILED>
 static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
                                  const CtaItem* items, int nitems, bool team, int max_lgN,
                                  const uint64_t* limbs, uint32_t* res, const uint2* twf,
@@ -1824,7 +1829,7 @@ static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
   const int Nmax = 1 << max_lgN;
   if (team) {
     const size_t smem = sizeof(uint32_t) * (size_t)(8 * kFwdThreads + (8 * kFwdThreads >> 5));
-    k_fwd2<D, true><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf, 0);
+    k_fwd2<D, true, TILED><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf, 0);
   } else {
     // whole-CTA transforms: the digit cache when the launch still fits
     // three CTAs an SM with it (every CTA's transform is at most Nmax)
@@ -1835,7 +1840,7 @@ static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
       smem += cache;
       dig_words = D * (Nmax >> 1);
     }
-    k_fwd2<D, false><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf,
+    k_fwd2<D, false, TILED><<<nitems, kFwdThreads, smem, st>>>(descs, idx, items, limbs, res, twf,
                                                         dig_words);
   }
   return cudaGetLastError();
@@ -1843,20 +1848,36 @@ static cudaError_t launch_fwd2_d(const FwdDesc* descs, const uint32_t* idx,
 
 int fwd_team_points() { return 8 * kFwdThreads; }
 
+template <bool TILED>
+static cudaError_t launch_fwd_items_t(const FwdDesc* descs, const uint32_t* idx,
+                                      const CtaItem* items, int nitems, int D, bool team,
+                                      int max_lgN, const uint64_t* limbs, uint32_t* res,
+                                      const uint2* twf, cudaStream_t st) {
+  switch (D) {
+#define MPZMM_FWD_CASE(DD) \
+  case DD:                 \
+    return launch_fwd2_d<DD, TILED>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
+    MPZMM_FWD_CASE(1)
+    MPZMM_FWD_CASE(2)
+    MPZMM_FWD_CASE(3)
+    MPZMM_FWD_CASE(4)
+    MPZMM_FWD_CASE(5)
+    MPZMM_FWD_CASE(6)
+    MPZMM_FWD_CASE(7)
+#undef MPZMM_FWD_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t launch_fwd_items(const FwdDesc* descs, const uint32_t* idx, const CtaItem* items,
                              int nitems, int D, bool team, int max_lgN, const uint64_t* limbs,
-                             uint32_t* res, const uint2* twf, cudaStream_t st) {
+                             uint32_t* res, const uint2* twf, cudaStream_t st, bool tiled) {
   if (nitems == 0) return cudaSuccess;
-  switch (D) {
-    case 1: return launch_fwd2_d<1>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 2: return launch_fwd2_d<2>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 3: return launch_fwd2_d<3>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 4: return launch_fwd2_d<4>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 5: return launch_fwd2_d<5>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 6: return launch_fwd2_d<6>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    case 7: return launch_fwd2_d<7>(descs, idx, items, nitems, team, max_lgN, limbs, res, twf, st);
-    default: return cudaErrorInvalidValue;
-  }
+  return tiled ? launch_fwd_items_t<true>(descs, idx, items, nitems, D, team, max_lgN, limbs, res,
+                                         twf, st)
+               : launch_fwd_items_t<false>(descs, idx, items, nitems, D, team, max_lgN, limbs,
+                                          res, twf, st);
 }
 
 cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const CtaItem* items,
@@ -1978,7 +1999,8 @@ int tc_smem_bytes(int m, int k, int n, int F, int bufcols) {
 // widest accumulator rounded up to a power of two (narrow products then
 // leave TMEM for a second CTA on the SM); F is the largest that lets as many
 // CTAs share an SM as TMEM allows (at most two), else the largest that fits.
-static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* F, int* smem) {
+static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* F, int* smem,
+                             bool* wide) {
   int widest = 0;
   for (int i = 0; i < nshapes; ++i) {
     const int c = tc::unit_cols(tc::shape_of(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]));
@@ -2002,6 +2024,7 @@ static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* 
       if (bytes <= limit && (target == 1 || f >= 4)) {
         *F = f;
         *smem = bytes;
+        *wide = target == 1;  // one CTA an SM: twice the threads
         return true;
       }
     }
@@ -2010,11 +2033,13 @@ static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* 
 }
 
 template <int F>
-static void launch_tc_f(int count, int smem, cudaStream_t st, const ProdDesc* prods,
+static void launch_tc_f(int count, int smem, bool wide, cudaStream_t st, const ProdDesc* prods,
                         const ContractItem* items, uint32_t* res, int bufcols, int* status,
                         int stall) {
-  k_contract_tc<F><<<count, tc::kThreads, smem, st>>>(prods, items, res, bufcols, status,
-                                                      stall);
+  if (wide)
+    k_contract_tc<F, 512><<<count, 512, smem, st>>>(prods, items, res, bufcols, status, stall);
+  else
+    k_contract_tc<F, 256><<<count, 256, smem, st>>>(prods, items, res, bufcols, status, stall);
 }
 
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
@@ -2025,13 +2050,15 @@ cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items,
     if (!contract_tc_eligible(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]))
       return cudaErrorInvalidValue;
   int F = 0, smem = 0, bufcols = 0;
-  if (!tc_launch_config(shapes, nshapes, &bufcols, &F, &smem)) return cudaErrorInvalidValue;
+  bool wide = false;
+  if (!tc_launch_config(shapes, nshapes, &bufcols, &F, &smem, &wide))
+    return cudaErrorInvalidValue;
   switch (F) {
-    case 16: launch_tc_f<16>(count, smem, st, prods, items, res, bufcols, status, stall); break;
-    case 8: launch_tc_f<8>(count, smem, st, prods, items, res, bufcols, status, stall); break;
-    case 4: launch_tc_f<4>(count, smem, st, prods, items, res, bufcols, status, stall); break;
-    case 2: launch_tc_f<2>(count, smem, st, prods, items, res, bufcols, status, stall); break;
-    default: launch_tc_f<1>(count, smem, st, prods, items, res, bufcols, status, stall); break;
+    case 16: launch_tc_f<16>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
+    case 8: launch_tc_f<8>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
+    case 4: launch_tc_f<4>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
+    case 2: launch_tc_f<2>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
+    default: launch_tc_f<1>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
   }
   return cudaGetLastError();
 }
@@ -2120,10 +2147,13 @@ template <int D>
 static cudaError_t set_fwd_attrs() {
   const int big =
       (int)(sizeof(uint32_t) * ((1 << kMaxLgNOneCta) + ((1 << kMaxLgNOneCta) >> 5)));
-  cudaError_t e = cudaFuncSetAttribute(k_fwd2<D, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_fwd2<D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaError_t e;
+  for (auto fn : {k_fwd2<D, true, false>, k_fwd2<D, false, false>, k_fwd2<D, true, true>,
+                  k_fwd2<D, false, true>})
+    if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) !=
+        cudaSuccess)
+      return e;
+  return cudaSuccess;
 }
 
 template <int P>
@@ -2169,8 +2199,10 @@ cudaError_t init_kernel_attributes() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
           cudaSuccess)
     return e;
-  for (auto fn : {k_contract_tc<16>, k_contract_tc<8>, k_contract_tc<4>, k_contract_tc<2>,
-                  k_contract_tc<1>})
+  for (auto fn : {k_contract_tc<16, 256>, k_contract_tc<8, 256>, k_contract_tc<4, 256>,
+                  k_contract_tc<2, 256>, k_contract_tc<1, 256>, k_contract_tc<16, 512>,
+                  k_contract_tc<8, 512>, k_contract_tc<4, 512>, k_contract_tc<2, 512>,
+                  k_contract_tc<1, 512>})
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   tc::kDynSmemLimit)) != cudaSuccess)
       return e;

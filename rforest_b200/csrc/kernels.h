@@ -24,9 +24,12 @@ cudaError_t launch_inv_ntt(const InvDesc* descs, const uint32_t* idx, int count,
 // (several entries per CTA); otherwise one entry per CTA and max_lgN sizes
 // the shared memory.  D = digits of 30 bits of the widest coefficient.
 int fwd_team_points();
+// tiled: the launch's entries are operands of tensor-core products, written
+// in the frequency-blocked layout (FwdDesc::tile_np); else the plain layout.
 cudaError_t launch_fwd_items(const FwdDesc* descs, const uint32_t* idx, const CtaItem* items,
                              int nitems, int D, bool team, int max_lgN, const uint64_t* limbs,
-                             uint32_t* res, const uint2* twf, cudaStream_t st);
+                             uint32_t* res, const uint2* twf, cudaStream_t st,
+                             bool tiled = false);
 cudaError_t launch_inv_items(const InvDesc* descs, const uint32_t* idx, const CtaItem* items,
                              int nitems, bool team, int max_lgN, uint32_t* res,
                              const uint2* twi, cudaStream_t st);
