@@ -717,7 +717,7 @@ def serving_benchmark(api, args):
     plain = len(trip) / (time.perf_counter() - t0)
     out["plain_one_call_per_request"] = {"value": plain, "unit": "requests/s",
                                          "note": "mpzmm_matmul per request, same pool"}
-    slots, max_batch, window = 3, 32, 200
+    slots, max_batch, window = 6, 32, 200
     srv = api.Server(slots=slots, max_batch=max_batch, window_us=window)
     out["server_config"] = {"slots": slots, "max_batch": max_batch, "window_us": window,
                             "budget": "3/4 of free memory"}

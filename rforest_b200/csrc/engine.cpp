@@ -351,7 +351,12 @@ int Workspace::reserve(size_t limbs, size_t res, size_t out_words, size_t sizes,
   auto grow_host = [&](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
     if (cap) want = grown(want, cap);
-    if (*p) cudaFreeHost(*p);
+    if (*p) {
+      if (retire_host)
+        retired_host.push_back(*p);
+      else
+        cudaFreeHost(*p);
+    }
     *p = nullptr;
     cap = 0;
     if (take_test_fail_alloc())
@@ -417,6 +422,8 @@ void Workspace::release_device() {
 
 void Workspace::release() {
   release_device();
+  for (void* p : retired_host) cudaFreeHost(p);
+  retired_host.clear();
   cudaFreeHost(h_limbs);
   cudaFreeHost(h_out);
   cudaFreeHost(h_sizes);
@@ -430,18 +437,34 @@ void Workspace::release() {
   hcap_limbs = hcap_out = hcap_sizes = hcap_desc = 0;
 }
 
+// Largest bit length among entries: only the longest entries can hold it,
+// so only their top limbs are read (each a likely cache miss) unless none of
+// them is normalised.
+static int64_t max_bits(const std::vector<EntryRef>& ents, int64_t* limbs) {
+  int64_t max_nl = 0, bits = 0;
+  for (const auto& e : ents) {
+    const int64_t nl = e.size < 0 ? -(int64_t)e.size : e.size;
+    *limbs += nl;
+    if (nl > max_nl) max_nl = nl;
+  }
+  if (!max_nl) return 0;
+  for (const auto& e : ents)
+    if ((e.size < 0 ? -(int64_t)e.size : e.size) == max_nl) {
+      const int64_t b = bit_length(e);
+      if (b > bits) bits = b;
+    }
+  if (bits <= 64 * (max_nl - 1))
+    for (const auto& e : ents) {
+      const int64_t b = bit_length(e);
+      if (b > bits) bits = b;
+    }
+  return bits;
+}
+
 int64_t estimate_device_bytes(const ProductSpec& ps, int64_t* host_bytes) {
-  int64_t a_bits = 0, b_bits = 0, limbs = 0;
-  for (const auto& e : ps.a) {
-    const int64_t b = bit_length(e);
-    if (b > a_bits) a_bits = b;
-    limbs += e.size < 0 ? -(int64_t)e.size : e.size;
-  }
-  for (const auto& e : ps.b) {
-    const int64_t b = bit_length(e);
-    if (b > b_bits) b_bits = b;
-    limbs += e.size < 0 ? -(int64_t)e.size : e.size;
-  }
+  int64_t limbs = 0;
+  const int64_t a_bits = max_bits(ps.a, &limbs);
+  const int64_t b_bits = max_bits(ps.b, &limbs);
   Params prm;
   if (!choose_params(a_bits, b_bits, ps.m, ps.k, ps.n, &prm)) return -1;
   const int64_t entries = (int64_t)ps.m * ps.k + (int64_t)ps.k * ps.n + (int64_t)ps.m * ps.n;
@@ -453,9 +476,14 @@ int64_t estimate_device_bytes(const ProductSpec& ps, int64_t* host_bytes) {
 }
 
 int Workspace::reserve_staging(size_t stage_limbs, size_t stage_out_words) {
-  auto grow = [](auto** p, size_t& cap, size_t want, size_t elem) -> int {
+  auto grow = [this](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
-    if (*p) cudaFreeHost(*p);
+    if (*p) {
+      if (retire_host)
+        retired_host.push_back(*p);
+      else
+        cudaFreeHost(*p);
+    }
     *p = nullptr;
     cap = 0;
     if (take_test_fail_alloc())

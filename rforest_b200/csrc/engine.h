@@ -97,6 +97,11 @@ struct Workspace {
   // the device's default pool.  Nothing then synchronises the device.
   cudaStream_t async_stream = nullptr;
   cudaMemPool_t pool = nullptr;
+  // Pinned staging outgrown by a later batch: kept here and freed only by
+  // release() when retire_host is set (cudaFreeHost synchronises the whole
+  // device, which would stall every other batch in flight).
+  bool retire_host = false;
+  std::vector<void*> retired_host;
   // Ensures room for the given element counts (device buffers, then the
   // pinned staging of limbs and output words); returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,

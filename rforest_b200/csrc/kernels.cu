@@ -402,8 +402,9 @@ __device__ __forceinline__ uint32_t digits_residue(const uint32_t (&dg)[D], int 
 
 // Where the forward transform leaves point h of prime j of an entry: the
 // plain frequency-contiguous layout (base + j N + h), or, for an operand of a
-// tensor-core product, blocked by kTcTile frequencies across the operand's
-// np entries (base + ((j N / 4 + h / 4) np + e) 4 + h mod 4).
+// tensor-core product, blocked by kTcTile = 8 frequencies (a 32-byte sector)
+// across the operand's np entries (base + ((j N / 8 + h / 8) np + e) 8 +
+// h mod 8).
 // TILED is a template flag so that plain launches carry none of the
 // blocked layout's state.
 template <bool TILED>
@@ -413,17 +414,17 @@ struct FwdOut {
   int lgN;
   __device__ __forceinline__ uint32_t* at(int j, uint32_t h) const {
     if (!TILED) return base + ((uint64_t)j << lgN) + h;
-    const uint64_t tile = ((uint64_t)j << (lgN - 2)) + (h >> 2);
-    return base + (tile * np + e) * (uint64_t)kTcTile + (h & 3u);
+    const uint64_t tile = ((uint64_t)j << (lgN - kTcTileLg)) + (h >> kTcTileLg);
+    return base + (tile * np + e) * (uint64_t)kTcTile + (h & (kTcTile - 1u));
   }
 };
 
 // 2^L consecutive points h0 .. (h0 a multiple of 2^L) reduced from [0, 4p)
-// to [0, p), vector stores (a 4-point run never crosses a block)
+// to [0, p), vector stores (a run of up to 8 points never crosses a block)
 template <int L, bool TILED>
 __device__ __forceinline__ void store_points(const FwdOut<TILED>& fo, int j, uint32_t h0,
                                              uint32_t* a, uint32_t p) {
-  static_assert(kTcTile == 4, "vector stores assume 4-frequency blocks");
+  static_assert(kTcTile == 8, "vector stores assume 8-frequency blocks");
   const uint32_t p2 = 2 * p;
 #pragma unroll
   for (int q = 0; q < (1 << L); ++q) {
@@ -1338,18 +1339,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
 
 // F consecutive residues (frequencies hs .. hs + F - 1) of entry e of an
 // operand stored in the blocked layout (FwdOut): blk is the operand block, np
-// its entries, tile the block of frequency hs (prime j included: j N/4 +
-// hs/4).  Only nf of them exist when the transform is shorter than the
-// CTA's frequencies.  Lanes take consecutive entries, so a warp's loads are
-// one contiguous run per 4 frequencies.
+// its entries, tile the block of frequency hs (prime j included: j N/8 +
+// hs/8) and sub = hs mod 8.  Only nf of them exist when the transform is
+// shorter than the CTA's frequencies.  Lanes take consecutive entries, so a
+// warp's loads are one contiguous run per block.
 template <int F>
 __device__ __forceinline__ void load_freqs(const uint32_t* __restrict__ blk, uint64_t np,
                                            uint64_t e, uint64_t tile, uint32_t sub, bool ok,
                                            int nf, uint32_t (&x)[F]) {
-  if (ok && nf == F && F >= 4) {  // sub == 0: F / 4 whole blocks
+  if (ok && nf == F && F >= 4) {  // sub is a multiple of 4: 16-byte pieces of blocks
 #pragma unroll
     for (int c = 0; c < F / 4; ++c) {
-      const uint4 u = __ldg(reinterpret_cast<const uint4*>(blk + ((tile + c) * np + e) * 4));
+      const uint32_t h = sub + 4u * (uint32_t)c;
+      const uint4 u = __ldg(reinterpret_cast<const uint4*>(
+          blk + ((tile + (h >> kTcTileLg)) * np + e) * kTcTile + (h & (kTcTile - 1u))));
       x[4 * c] = u.x;
       x[4 * c + 1] = u.y;
       x[4 * c + 2] = u.z;
@@ -1359,7 +1362,9 @@ __device__ __forceinline__ void load_freqs(const uint32_t* __restrict__ blk, uin
 #pragma unroll
     for (int f = 0; f < F; ++f) {
       const uint32_t h = sub + (uint32_t)f;
-      x[f] = (ok && f < nf) ? __ldg(blk + ((tile + (h >> 2)) * np + e) * 4 + (h & 3u)) : 0u;
+      x[f] = (ok && f < nf) ? __ldg(blk + ((tile + (h >> kTcTileLg)) * np + e) * kTcTile +
+                                    (h & (kTcTile - 1u)))
+                            : 0u;
     }
   }
 }
@@ -1429,8 +1434,8 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     const int nf = (int)((uint32_t)N - hs < (uint32_t)F ? (uint32_t)N - hs : (uint32_t)F);
     const uint64_t base = (uint64_t)j * (uint64_t)N + hs;
     // the operands' blocked layout: frequency block of hs, offset inside it
-    const uint64_t tile0 = ((uint64_t)j << (d.lgN - 2)) + (hs >> 2);
-    const uint32_t sub0 = hs & 3u;
+    const uint64_t tile0 = ((uint64_t)j << (d.lgN - kTcTileLg)) + (hs >> kTcTileLg);
+    const uint32_t sub0 = hs & (kTcTile - 1u);
 
     // ---- stage A' and B' of the nf frequencies: a warp task is 8 rows
     // (i of A, l of B) by 16 terms; a thread gathers four terms' residues

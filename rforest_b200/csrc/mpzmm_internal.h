@@ -88,7 +88,8 @@ struct FwdDesc {
   uint32_t tile_np = 0;
   uint32_t tile_e = 0;
 };
-constexpr int kTcTile = 4;  // frequencies a block of the tensor-core layout
+constexpr int kTcTile = 8;      // frequencies a block of the tensor-core layout (32 bytes)
+constexpr int kTcTileLg = 3;
 
 // One output polynomial of the inverse transform + CRT + recompose.
 struct InvDesc {

@@ -247,6 +247,7 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
     }
     sl->ws.async_stream = sl->stream;
     sl->ws.pool = s->pool;
+    sl->ws.retire_host = true;
     s->slots.push_back(std::move(sl));
   }
   mpzmm_server* raw = s.get();

@@ -106,3 +106,20 @@ def test_plan_graph_replay_with_new_inputs(gpu):
         want.append(PK.digest(api.matmul(p.m, p.k, p.n, A, B)))
     assert second == want
     plan.close()
+
+
+def test_server_admission_window(gpu):
+    """The admission window changes how requests are batched, never the
+    results; a negative window is refused."""
+    reqs = small_requests(24, seed=41)
+    alone = [PK.digest(api.matmul(p.m, p.k, p.n, p.A, p.B)) for p in reqs]
+    for window in (0, 2000):
+        srv = api.Server(slots=2, max_batch=8, window_us=window)
+        try:
+            tickets = [srv.submit(p.m, p.k, p.n, p.A, p.B) for p in reqs]
+            assert [PK.digest(srv.wait(t, 60000)) for t in tickets] == alone
+            with pytest.raises(_lib.MpzmmError) as e:
+                srv.set_admission_window(-1)
+            assert e.value.status == _lib.MPZMM_ERR_ARG
+        finally:
+            srv.close()
