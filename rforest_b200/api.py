@@ -208,7 +208,17 @@ class _Holder:
 
 def matmul(m: int, k: int, n: int, A: Packed, B: Packed, stream=None) -> Packed:
     """Exact C = A * B (A m x k, B k x n, row-major packed vectors)."""
-    h = _Holder(m, k, n, A, B)
+    return matmul_holder(_Holder(m, k, n, A, B), stream)
+
+
+def holder(m: int, k: int, n: int, A: Packed, B: Packed) -> "_Holder":
+    """The arrays of one product laid out for the C ABI (inputs, result
+    arrays sized by the library's bound), reusable for repeated calls."""
+    return _Holder(m, k, n, A, B)
+
+
+def matmul_holder(h: "_Holder", stream=None) -> Packed:
+    """mpzmm_matmul on a holder's arrays; the result is a view of them."""
     _lib.check(_lib.lib().mpzmm_matmul_batch(1, C.byref(h.struct), _stream_arg(stream)))
     return h.result()
 
@@ -413,7 +423,11 @@ class Server:
         _lib.check(_lib.lib().mpzmm_server_set_admission_window(self.handle, int(microseconds)))
 
     def submit(self, m: int, k: int, n: int, A: Packed, B: Packed) -> int:
-        h = _Holder(m, k, n, A, B)
+        return self.submit_holder(_Holder(m, k, n, A, B))
+
+    def submit_holder(self, h: "_Holder") -> int:
+        """Queues a request whose arrays are already laid out (a holder made
+        once and reused once its previous request has completed)."""
         t = C.c_uint64()
         _lib.check(_lib.lib().mpzmm_server_submit(self.handle, C.byref(h.struct), C.byref(t)))
         self.holders[t.value] = h

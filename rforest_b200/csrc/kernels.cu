@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "kernels.h"
 #include "modarith.cuh"
@@ -2013,6 +2014,15 @@ static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* 
   }
   int b = 32;
   while (b < widest) b <<= 1;
+  // tuning: a wider buffer groups more frequencies of narrow products per
+  // commit at the cost of the second CTA on the SM (MPZMM_TC_BUFCOLS, a
+  // power of two up to 256)
+  static const int b_env = [] {
+    const char* e = std::getenv("MPZMM_TC_BUFCOLS");
+    const int v = e ? std::atoi(e) : 0;
+    return (v >= 32 && v <= 256 && (v & (v - 1)) == 0) ? v : 0;
+  }();
+  if (b_env > b) b = b_env;
   *bufcols = b;
   const int tcols = tc::double_buffered(b) ? 2 * b : b;
   const int per_sm = 512 / tcols >= 2 ? 2 : 1;
