@@ -6,29 +6,32 @@
 //     sum_kk A[i,kk] B[kk,l] = sum_{s,t} 2^(8(s+t)) D_st[i,l],
 //     D_st[i,l] = sum_kk a_s[i,kk] b_t[kk,l]      (0 <= D < k 2^16, exact in int32),
 // sixteen byte-plane products that one u8 x u8 GEMM computes at once:
-//   A' rows s m8 + i   (the four byte planes of A stacked along M, m8 = m
-//                       rounded up to 32, 64 or 128 rows a plane), bytes kk;
+//   A' rows 4 i + s    (the four byte planes of A interleaved along M, in
+//                       tiles of 128 rows = 32 rows i), bytes kk;
 //   B' rows 4 l + t    (the planes of B interleaved along N), bytes kk;
-//   D = A' B'^T        (M = 4 m8 in tiles of 128 TMEM lanes, N = 4 n).
+//   D = A' B'^T        (M = 4 m in tiles of 128 TMEM lanes, N = 4 n).
 // Half the MACs of a Toeplitz-expanded split and no expansion of either
-// operand: the split is four byte permutes per four residues.  The epilogue
-// forms z = sum_{s,t} (2^(8(s+t)) mod p) D_st (< 2^57 for k <= 64) in 64 bits,
-// adding the partial sums of the lanes that hold the same row i, and
-// Montgomery-reduces it, so C carries the same 2^-32 factor as the CUDA-core
-// contraction.
+// operand: the split is four byte permutes per four residues.  The four
+// planes of row i sit in four adjacent TMEM lanes, so one warp holds them:
+// the epilogue weights a lane's sixteen values by 2^(8(s+t)) mod p in 64
+// bits, adds the four lanes' sums with three shuffles (z < 2^57 for
+// k <= 64) and Montgomery-reduces z, so C carries the same 2^-32 factor as
+// the CUDA-core contraction.  Small products pack two or four frequencies
+// into one MMA (Shape).
 //
-// One CTA of 256 threads (512 where it has the SM to itself) per (product,
-// prime, block of 128 frequencies),
+// One CTA of 128, 256 or 512 threads (four, two or one an SM, as TMEM and
+// shared memory allow) per (product, prime, block of 128 frequencies),
 // processed F frequencies at a time: all warps stage A' and B' of the F
 // frequencies straight from global memory (F consecutive residues of a
 // polynomial per vector load) into canonical K-major no-swizzle tiles (8-row
 // x 16-byte core matrices; every st.shared of a warp hits 32 distinct
-// banks); one thread issues the MMAs of a unit (several frequencies of a
+// banks); one thread issues the MMAs of a unit (several groups of a
 // product with at most 32 output columns, else one frequency's 32 columns),
-// tcgen05.commit arrives on the unit's mbarrier; with two 256-column TMEM
-// buffers the next unit's MMAs run while all eight warps drain the
-// current one (warp w reads TMEM lanes 32 (w mod 4) .. + 31, the
-// warpgroups take turns at 16-column chunks).  Results of the F
+// tcgen05.commit arrives on the unit's mbarrier, which one warp waits for
+// before a block barrier releases the rest; with two TMEM buffers the
+// next unit's MMAs run while the warps drain the current one (warp w reads
+// TMEM lanes 32 (w mod 4) .. + 31; warps whose lanes hold no row skip the
+// unit).  Results of the F
 // frequencies are gathered in shared memory and stored F residues per vector
 // store.  Every wait is bounded (one second of wall time): on time-out the
 // CTA records an error, waits (bounded) for MMAs it has issued, frees its
@@ -40,7 +43,6 @@
 namespace mpzmm {
 namespace tc {
 
-constexpr int kThreads = 256;    // threads of a CTA that shares its SM (512 alone)
 constexpr int kMaxK = 64;        // k <= 64: K' = k bytes padded to 32, z < 2^57
 constexpr int kMaxN = 64;        // n <= 64: at most two units of 32 outputs a frequency
 constexpr int kMaxM = 128;       // m <= 128: four planes in four 128-lane tiles
@@ -52,38 +54,47 @@ constexpr int kSmemLimit = 227 * 1024;  // shared memory of a block, static incl
 constexpr int kStaticSmem = 1024;       // the kernel's barriers and TMEM slot (aligned)
 constexpr int kDynSmemLimit = kSmemLimit - kStaticSmem;
 
-// Shape of one product on the tensor cores (host and device).
+// Shape of one product on the tensor cores (host and device) when F
+// frequencies are staged at once.  Products with at most 16 rows and 32
+// columns pack phi frequencies into one 128-row M tile (a group): slot fl
+// holds rows 4 mp fl + 4 i + s of A' and bytes fl kq .. fl kq + kq of K'
+// in both A' and B', and A' is zero outside its slot, so the one MMA gives
+// each frequency's sixteen plane products in its own rows; the groups of a
+// block then fill all four TMEM lane quadrants instead of the first one or
+// two.
 struct Shape {
-  int m8;      // rows per plane: 32, 64 or 128
-  int mt;      // 128-lane M tiles: 4 m8 / 128
-  int kp;      // K' bytes: k rounded up to 32
+  int phi;     // frequencies a group: 4 (m <= 8), 2 (m <= 16), else 1; at most F
+  int mp;      // rows i a packed slot spans: 8 or 16 (32 when phi = 1)
+  int mt;      // 128-lane M tiles of a group: 1 when packed, else ceil(m / 32)
+  int kq;      // K' bytes of a slot: k rounded up to 8 when packed, to 32 when not
+  int kp;      // K' bytes of a group: phi kq rounded up to 32
   int npl;     // output columns per unit: min(n, 32)
-  int nunits;  // units per frequency: ceil(n / npl)
+  int nunits;  // units per frequency: ceil(n / npl) (1 when packed)
   int ncol;    // MMA N of a unit: 4 npl rounded up to 16
-  int g;       // lanes holding one row i: 128 / m8
-  int a_bytes, b_bytes, red_bytes;
+  int a_bytes, b_bytes;  // A' and B' tiles of one group
 };
 
-__host__ __device__ inline Shape shape_of(int m, int k, int n) {
+__host__ __device__ inline Shape shape_of(int m, int k, int n, int F) {
   Shape s;
-  s.m8 = m <= 32 ? 32 : (m <= 64 ? 64 : 128);
-  s.mt = 4 * s.m8 / 128;
-  s.kp = (k + 31) & ~31;
+  s.phi = n > kUnitCols ? 1 : (m <= 8 ? 4 : (m <= 16 ? 2 : 1));
+  if (s.phi > F) s.phi = F;
+  s.mp = s.phi > 1 ? (m <= 8 ? 8 : 16) : 32;
+  s.mt = s.phi > 1 ? 1 : (m + 31) / 32;
+  s.kq = s.phi > 1 ? (k + 7) & ~7 : (k + 31) & ~31;
+  s.kp = (s.phi * s.kq + 31) & ~31;
   s.npl = n < kUnitCols ? n : kUnitCols;
   s.nunits = (n + s.npl - 1) / s.npl;
   s.ncol = (4 * s.npl + 15) & ~15;
-  s.g = 128 / s.m8;
-  s.a_bytes = 4 * s.m8 * s.kp;  // multiple of 4096
+  s.a_bytes = 128 * s.mt * s.kp;  // multiple of 4096
   // B' rows: every unit's MMA reads ncol rows from row 4 npl u, and the
   // staging writes rows 4 l + t for l up to n rounded up to 8
   int brows = 4 * s.npl * (s.nunits - 1) + s.ncol;
   if (brows < 4 * ((n + 7) & ~7)) brows = 4 * ((n + 7) & ~7);
   s.b_bytes = ((brows * s.kp) + 1023) & ~1023;
-  s.red_bytes = s.g > 1 ? 128 * (s.npl + 1) * 8 : 0;
   return s;
 }
 
-// TMEM columns of one frequency's accumulator (one column range).
+// TMEM columns of one group's accumulator (one column range).
 __host__ __device__ inline int unit_cols(const Shape& s) { return s.mt * s.ncol; }
 
 // A launch keeps two accumulator buffers of `bufcols` TMEM columns (a power
@@ -91,13 +102,14 @@ __host__ __device__ inline int unit_cols(const Shape& s) { return s.mt * s.ncol;
 // the 512 columns of an SM, one otherwise.
 __host__ __device__ inline bool double_buffered(int bufcols) { return 2 * bufcols <= 512; }
 
-// Frequencies per unit when F are staged: products with one column range
-// (n <= 32) put that many frequencies' accumulators side by side in a
+// Groups per unit when F frequencies are staged: products with one column
+// range (n <= 32) put that many groups' accumulators side by side in a
 // buffer, so one commit and one epilogue pass serve them all.
 __host__ __device__ inline int group_freqs(const Shape& s, int F, int bufcols) {
   if (s.nunits != 1) return 1;
+  const int groups = F / s.phi;
   int g = bufcols / unit_cols(s);
-  return g < 1 ? 1 : (g > F ? F : g);
+  return g < 1 ? 1 : (g > groups ? groups : g);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -1307,19 +1307,18 @@ __device__ __forceinline__ void tc_commit(uint32_t barp) {
                :: "r"(barp) : "memory");
 }
 
-// The MMAs of unit u (frequency u / nunits of the staged block, output
-// columns npl (u mod nunits) ..) into the accumulator at TMEM column dcol:
-// one M tile of 128 A' rows at a time, K' in steps of 32 bytes.
+// The MMAs of group gu / nunits of the staged block, output columns
+// npl (gu mod nunits) .., into the accumulator at TMEM column dcol: one M
+// tile of 128 A' rows at a time, K' in steps of 32 bytes.
 __device__ __forceinline__ void tc_issue_unit(const tc::Shape& sh, uint32_t a_base,
-                                              uint32_t b_base, int u, uint32_t dcol) {
-  const int f = u / sh.nunits;
-  const int uu = u - f * sh.nunits;
+                                              uint32_t b_base, int gu, uint32_t dcol) {
+  const int g = gu / sh.nunits;
+  const int uu = gu - g * sh.nunits;
   const uint32_t kp = (uint32_t)sh.kp;
-  const uint32_t a0 = a_base + (uint32_t)(f * sh.a_bytes);
+  const uint32_t a0 = a_base + (uint32_t)(g * sh.a_bytes);
   // B' row 4 npl uu (a multiple of 8: npl = 32 when there are several units)
-  const uint32_t b0 = b_base + (uint32_t)(f * sh.b_bytes) + (uint32_t)(4 * sh.npl * uu) * kp;
+  const uint32_t b0 = b_base + (uint32_t)(g * sh.b_bytes) + (uint32_t)(4 * sh.npl * uu) * kp;
   const uint32_t idesc = tc::idesc_u8((uint32_t)sh.ncol);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   for (int q = 0; q < sh.mt; ++q)
     for (uint32_t ks = 0; ks < kp / 32; ++ks)
       tc_mma(dcol + (uint32_t)(q * sh.ncol),
@@ -1370,8 +1369,8 @@ __device__ __forceinline__ void load_freqs(const uint32_t* __restrict__ blk, uin
   }
 }
 
-// NT threads: 256 where two CTAs share an SM, 512 where one CTA has it to
-// itself (more warps to cover the staging and epilogue latency).
+// NT threads: 128 where four CTAs share an SM (one warp a TMEM lane
+// quadrant), 256 where two do, 512 where one CTA has it to itself.
 template <int F, int NT>
 __global__ void __launch_bounds__(NT, 512 / NT)
 k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ items,
@@ -1391,22 +1390,33 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   const uint32_t pinv = c_primes[j].pinv;
   const uint32_t mu = c_primes[j].mu;
   const uint64_t stride = (uint64_t)d.P * (uint64_t)N;
-  const tc::Shape sh = tc::shape_of(m, k, n);
+  const tc::Shape sh = tc::shape_of(m, k, n, F);
+  const int phi = sh.phi;
+  const int G = F / phi;  // groups of a staged block
   const bool dbl = tc::double_buffered(bufcols);
   const int tmem_cols = dbl ? 2 * bufcols : bufcols;
   const uint32_t ucols = (uint32_t)tc::unit_cols(sh);
-  // frequencies per unit: products with one column range put several
-  // frequencies' accumulators side by side in a TMEM buffer
+  // groups per unit: products with one column range put several groups'
+  // accumulators side by side in a TMEM buffer
   const int gf = tc::group_freqs(sh, F, bufcols);
-  const int plane_bytes = sh.m8 * sh.kp;
   uint8_t* As = tsm;
-  uint8_t* Bs = As + F * sh.a_bytes;
-  uint64_t* red = reinterpret_cast<uint64_t*>(Bs + F * sh.b_bytes);
-  uint32_t* outs =
-      reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(red) + gf * sh.red_bytes);
+  uint8_t* Bs = As + G * sh.a_bytes;
+  // results of the staged frequencies, F + 1 words an output entry (odd
+  // stride: the epilogue's scattered stores spread over the banks)
+  uint32_t* outs = reinterpret_cast<uint32_t*>(Bs + G * sh.b_bytes);
+  // this lane's byte plane s of A (rows 4 i + s) and its four weights
+  // 2^(8(s+t)) mod p, t = 0..3
+  uint32_t wt[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) wt[t] = (uint32_t)c_primes[j].w8[(lane & 3) + t];
   const uint32_t a_base = tc::smem_u32(As), b_base = tc::smem_u32(Bs);
   const uint32_t barp[2] = {tc::smem_u32(&bars[0]), tc::smem_u32(&bars[1])};
 
+  // packed groups: A' is zero outside each slot's K' bytes; the staging
+  // writes only inside the slots, so the zeros stay for the whole CTA
+  if (phi > 1)
+    for (int x = tid; x < G * sh.a_bytes / 16; x += NT)
+      reinterpret_cast<uint4*>(As)[x] = make_uint4(0u, 0u, 0u, 0u);
   if (warp == 0) {
     const uint32_t slot = tc::smem_u32(&tmem_slot);
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -1428,6 +1438,11 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   int pending[2] = {0, 0};
   bool failed = false;
   const int issue_mma = stall ? 0 : 1;  // stall (failure-path tests only): no MMA, no commit
+  // this warp's TMEM lanes 32 qd + lane of every M tile: packed slot fl and
+  // first row i (ib0 + 32 q; lane / 4 is added)
+  const int qd = warp & 3;
+  const int fl = phi > 1 ? (32 * qd) / (4 * sh.mp) : 0;
+  const int ib0 = phi > 1 ? ((32 * qd) % (4 * sh.mp)) / 4 : 8 * qd;
 
   for (int fb0 = 0; fb0 < tc::kFreqs; fb0 += F) {
     const uint32_t hs = it.h0 + (uint32_t)fb0;
@@ -1439,10 +1454,10 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     const uint32_t sub0 = hs & (kTcTile - 1u);
 
     // ---- stage A' and B' of the nf frequencies: a warp task is 8 rows
-    // (i of A, l of B) by 16 terms; a thread gathers four terms' residues
-    // of one row for every frequency and writes their byte planes.  Small F
-    // keeps TU tasks' loads in flight at once.
-    const int kbn = sh.kp / 16;
+    // (i of A, l of B) by 16 terms of a slot; a thread gathers four terms'
+    // residues of one row for every frequency and writes their byte planes.
+    // Small F keeps TU tasks' loads in flight at once.
+    const int kbn = (sh.kq + 15) / 16;
     const int a_tasks = ((m + 7) / 8) * kbn;
     const int tasks = a_tasks + ((n + 7) / 8) * kbn;
     constexpr int TU = F <= 4 ? 2 : 1;
@@ -1460,8 +1475,8 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
         const int rb = tt / kbn;
         const int kb = tt - rb * kbn;
         const int kk0 = 16 * kb + 4 * (lane & 3);
-        // A: lane -> (row i mod 8, term quad); B: lane -> (l mod 8, term quad)
-        const int r = 8 * rb + (isA ? ((lane >> 2) & 7) : (lane >> 2));
+        // lane -> (row i of A or column l of B mod 8, term quad)
+        const int r = 8 * rb + (lane >> 2);
         rr[w2] = r;
         kq[w2] = kk0;
         isa[w2] = isA;
@@ -1479,31 +1494,27 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
       for (int w2 = 0; w2 < TU; ++w2) {
         if (task0 + w2 * kWarps >= tasks) break;  // uniform over the warp
         const int r = rr[w2], kk0 = kq[w2];
+        if (kk0 >= sh.kq) continue;  // past the slot (a packed slot of 8 or 24 bytes)
 #pragma unroll
         for (int f = 0; f < F; ++f) {
           if (f >= nf) break;
+          // frequency f: group f / phi, slot f mod phi
+          const int g = f / phi, sl = f - g * phi;
           uint32_t pl[4];
           tc::byte_planes(x[w2][0][f], x[w2][1][f], x[w2][2][f], x[w2][3][f], pl);
-          if (isa[w2]) {
-            // plane s of row i: rows s m8 + i; lanes cover (i mod 8, quad): no conflicts
-            uint8_t* t = As + f * sh.a_bytes + tc::tile_off((uint32_t)r, (uint32_t)kk0,
-                                                            (uint32_t)sh.kp);
+          // plane s of row i of A (column l of B): row 4 mp sl + 4 r + s of
+          // A' (4 r + s of B'), bytes sl kq + kk; the store order rotates
+          // with bits 3-4 of the lane so every store covers all 32 banks
+          uint8_t* t = isa[w2] ? As + g * sh.a_bytes : Bs + g * sh.b_bytes;
+          const uint32_t row0 = isa[w2] ? (uint32_t)(4 * sh.mp * sl + 4 * r) : (uint32_t)(4 * r);
+          const uint32_t kb = (uint32_t)(sl * sh.kq + kk0);
+          const int gq = (lane >> 3) & 3;
 #pragma unroll
-            for (int s2 = 0; s2 < 4; ++s2)
-              *reinterpret_cast<uint32_t*>(t + s2 * plane_bytes) = pl[s2];
-          } else {
-            // plane t of column l: row 4 l + t; the store order rotates with
-            // bits 3-4 of the lane so every store covers all 32 banks
-            uint8_t* t = Bs + f * sh.b_bytes;
-            const int g = (lane >> 3) & 3;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int tp = (q + g) & 3;
-              const uint32_t v =
-                  tp == 0 ? pl[0] : (tp == 1 ? pl[1] : (tp == 2 ? pl[2] : pl[3]));
-              *reinterpret_cast<uint32_t*>(
-                  t + tc::tile_off((uint32_t)(4 * r + tp), (uint32_t)kk0, (uint32_t)sh.kp)) = v;
-            }
+          for (int q = 0; q < 4; ++q) {
+            const int tp = (q + gq) & 3;
+            const uint32_t v = tp == 0 ? pl[0] : (tp == 1 ? pl[1] : (tp == 2 ? pl[2] : pl[3]));
+            *reinterpret_cast<uint32_t*>(t + tc::tile_off(row0 + (uint32_t)tp, kb,
+                                                          (uint32_t)sh.kp)) = v;
           }
         }
       }
@@ -1511,36 +1522,56 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
 
-    // ---- units: MMAs, then the epilogue of each.  A unit is gf
-    // frequencies (products with one column range) or one frequency's
-    // column range uu; its accumulators are consecutive in TMEM ----
-    const int U = sh.nunits == 1 ? (nf + gf - 1) / gf : nf * sh.nunits;
-    auto unit_freqs = [&](int u, int* f0, int* nfu, int* uu) {
+    // ---- units: MMAs, then the epilogue of each.  A unit is gf groups
+    // (products with one column range) or one frequency's column range uu;
+    // its accumulators are consecutive in TMEM ----
+    const int ng = (nf + phi - 1) / phi;  // groups holding staged frequencies
+    const int U = sh.nunits == 1 ? (ng + gf - 1) / gf : nf * sh.nunits;
+    auto unit_groups = [&](int u, int* g0, int* ngu, int* uu) {
       if (sh.nunits == 1) {
-        *f0 = u * gf;
-        *nfu = (nf - *f0) < gf ? (nf - *f0) : gf;
+        *g0 = u * gf;
+        *ngu = (ng - *g0) < gf ? (ng - *g0) : gf;
         *uu = 0;
       } else {
-        *f0 = u / sh.nunits;
-        *nfu = 1;
-        *uu = u - *f0 * sh.nunits;
+        *g0 = u / sh.nunits;
+        *ngu = 1;
+        *uu = u - *g0 * sh.nunits;
       }
     };
     auto issue = [&](int u, uint32_t dcol) {
-      int f0, nfu, uu;
-      unit_freqs(u, &f0, &nfu, &uu);
-      for (int fi = 0; fi < nfu; ++fi)
-        tc_issue_unit(sh, a_base, b_base, (f0 + fi) * sh.nunits + uu,
-                      dcol + (uint32_t)fi * ucols);
+      int g0, ngu, uu;
+      unit_groups(u, &g0, &ngu, &uu);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int gi = 0; gi < ngu; ++gi)
+        tc_issue_unit(sh, a_base, b_base, (g0 + gi) * sh.nunits + uu,
+                      dcol + (uint32_t)gi * ucols);
     };
+    // both buffers are free at a block's start (every warp passed the last
+    // block's barriers after draining them): units 0 and 1 go at once
+    const bool two = dbl && U > 1;
     if (tid == 0 && issue_mma) {
       issue(0, tmem);
       tc_commit(barp[0]);
+      if (two) {
+        issue(1, tmem + (uint32_t)bufcols);
+        tc_commit(barp[1]);
+      }
     }
     pending[0] += issue_mma;
+    if (two) pending[1] += issue_mma;
     for (int u = 0; u < U; ++u) {
       const int buf = dbl ? (u & 1) : 0;
-      if (dbl && u + 1 < U) {  // the next unit's MMAs overlap this epilogue
+      // one warp waits for the unit's MMAs; the barrier releases the others
+      // and, with two buffers, tells that every warp has drained unit u - 1
+      const bool ok = warp == 0 ? tc::mbar_wait(barp[buf], phase[buf]) : true;
+      if (__syncthreads_or(!ok)) {  // every thread takes the same branch
+        failed = true;
+        break;
+      }
+      phase[buf] ^= 1u;
+      pending[buf] -= 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (dbl && u >= 1 && u + 1 < U) {  // into unit u - 1's buffer: overlaps this epilogue
         const int nb = (u + 1) & 1;
         if (tid == 0 && issue_mma) {
           issue(u + 1, tmem + (uint32_t)(nb * bufcols));
@@ -1548,74 +1579,49 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
         }
         pending[nb] += issue_mma;
       }
-      const bool ok = tc::mbar_wait(barp[buf], phase[buf]);
-      if (ok) {
-        phase[buf] ^= 1u;
-        pending[buf] -= 1;
-      }
-      if (__syncthreads_or(!ok)) {  // every thread takes the same branch
-        failed = true;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      int f0, nfu, uu;
-      unit_freqs(u, &f0, &nfu, &uu);
+      int g0, ngu, uu;
+      unit_groups(u, &g0, &ngu, &uu);
       const int l0 = uu * sh.npl;
       const int nl = (n - l0) < sh.npl ? (n - l0) : sh.npl;
       const int nch = (nl + 3) / 4;
-      const int qd = warp & 3;
-      const int lam = 32 * qd + lane;  // this thread's TMEM lane
-      const int i = lam % sh.m8;       // its row (the same in every M tile)
       const uint32_t laddr = tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(buf * bufcols);
-      for (int fi = 0; fi < nfu; ++fi) {
-        const int f = f0 + fi;
-        for (int ch = warp >> 2; ch < nch; ch += NT / 128) {  // warpgroups share the chunks
-          uint64_t part[4] = {0, 0, 0, 0};
-          for (int q = 0; q < sh.mt; ++q) {
-            uint32_t v[16];
-            tmem_ld16(laddr + (uint32_t)(fi * (int)ucols + q * sh.ncol + 16 * ch), v);
-            const int s = (128 * q + lam) / sh.m8;  // byte plane of this lane: warp-uniform
+      // the warps of quadrant qd share its (group, M tile, 16-column chunk)
+      // items; rows i of the quadrant in tile q: ib0 + 32 q + lane / 4
+      const int per_g = sh.mt * nch;
+      for (int xi = warp >> 2; xi < ngu * per_g; xi += NT / 128) {
+        const int gi = xi / per_g;
+        const int rem = xi - gi * per_g;
+        const int q = rem / nch;
+        const int ch = rem - q * nch;
+        const int f = (g0 + gi) * phi + fl;  // phi = 1 when nunits > 1
+        const int ib = ib0 + 32 * q;
+        if (fl >= phi || f >= nf || ib >= m) continue;  // warp-uniform: no row here
+        uint32_t v[16];
+        tmem_ld16(laddr + (uint32_t)(gi * (int)ucols + q * sh.ncol + 16 * ch), v);
+        // columns 4 c + t of the chunk: output l0 + 4 ch + c, B plane t
+        uint64_t part[4];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-              const uint64_t w = c_primes[j].w8[s + t];
-#pragma unroll
-              for (int u2 = 0; u2 < 4; ++u2) part[u2] += (uint64_t)v[4 * u2 + t] * w;
-            }
-          }
-          if (sh.g == 1) {  // all four planes of row i are in this lane
-            if (i < m) {
-#pragma unroll
-              for (int u2 = 0; u2 < 4; ++u2) {
-                const int l = 4 * ch + u2;
-                if (l < nl) outs[(i * n + l0 + l) * F + f] = redc64(part[u2], p, pinv, mu);
-              }
-            }
-          } else {
-            uint64_t* rf = red + fi * 128 * (sh.npl + 1);
-#pragma unroll
-            for (int u2 = 0; u2 < 4; ++u2) {
-              const int l = 4 * ch + u2;
-              if (l < nl) rf[lam * (sh.npl + 1) + l] = part[u2];
-            }
-          }
-        }
-      }
-      if (sh.g > 1) {  // add the partial sums of the g lanes that hold row i
-        __syncthreads();
-        const int per = m * nl;
-        for (int xo = tid; xo < nfu * per; xo += NT) {
-          const int fi = xo / per;
-          const int rem = xo - fi * per;
-          const int ii = rem / nl, l = rem - ii * nl;
-          const uint64_t* rf = red + fi * 128 * (sh.npl + 1);
+        for (int c = 0; c < 4; ++c) {
           uint64_t z = 0;
-          for (int g2 = 0; g2 < sh.g; ++g2) z += rf[(g2 * sh.m8 + ii) * (sh.npl + 1) + l];
-          outs[(ii * n + l0 + l) * F + f0 + fi] = redc64(z, p, pinv, mu);
+#pragma unroll
+          for (int t = 0; t < 4; ++t) z += (uint64_t)v[4 * c + t] * wt[t];
+          part[c] = z;
         }
+        // add over the four lanes of row i (planes s), lane s ending with
+        // output c = s: swap halves across lane bit 1, then across bit 0
+        const bool h1 = (lane & 2) != 0, h0 = (lane & 1) != 0;
+        uint64_t k0 = h1 ? part[2] : part[0], k1 = h1 ? part[3] : part[1];
+        k0 += __shfl_xor_sync(0xffffffffu, h1 ? part[0] : part[2], 2);
+        k1 += __shfl_xor_sync(0xffffffffu, h1 ? part[1] : part[3], 2);
+        uint64_t z = h0 ? k1 : k0;
+        z += __shfl_xor_sync(0xffffffffu, h0 ? k0 : k1, 1);
+        const int i = ib + (lane >> 2);
+        const int l = 4 * ch + (lane & 3);
+        if (i < m && l < nl) outs[(i * n + l0 + l) * (F + 1) + f] = redc64(z, p, pinv, mu);
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncthreads();
-      if (!dbl && u + 1 < U) {
+      if (!dbl && u + 1 < U) {  // one buffer: the next MMAs wait for every warp
+        __syncthreads();
         if (tid == 0 && issue_mma) {
           issue(u + 1, tmem);
           tc_commit(barp[0]);
@@ -1624,10 +1630,13 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
       }
     }
     if (failed) break;
-    // ---- the nf frequencies of every output, F residues a vector store ----
+    __syncthreads();  // every epilogue store of the block is in outs
+    // ---- the nf frequencies of every output, F residues a vector store.
+    // The next block's staging may start at once: this block's MMAs have
+    // all completed, and its epilogue writes outs only after its own barrier.
     for (int e = tid; e < m * n; e += NT) {
       uint32_t* dst = res + d.c_res + (uint64_t)e * stride + base;
-      const uint32_t* sv = outs + e * F;
+      const uint32_t* sv = outs + e * (F + 1);
       if (nf == F && F >= 4) {
 #pragma unroll
         for (int c = 0; c < F / 4; ++c)
@@ -1637,7 +1646,6 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
         for (int f = 0; f < nf; ++f) dst[f] = sv[f];
       }
     }
-    __syncthreads();  // before the next block overwrites tiles and results
   }
   if (failed) {
     if (tid == 0) atomicExch(status, 1);
@@ -1989,57 +1997,58 @@ bool contract_tc_eligible(int m, int k, int n) {
   return m >= 1 && m <= tc::kMaxM && k >= 1 && k <= tc::kMaxK && n >= 1 && n <= tc::kMaxN;
 }
 
-// Frequencies staged at once (F), dynamic shared memory and TMEM columns of a
-// tensor-core launch whose products have at most max_m rows, max_k terms and
-// max_n columns: per-product layouts are all within these bounds.
-// Dynamic shared memory of one product's CTA with F frequencies staged:
-// byte tiles, the lane-sum buffer of a unit, the results of the F frequencies.
-int tc_smem_bytes(int m, int k, int n, int F, int bufcols) {
-  const tc::Shape sh = tc::shape_of(m, k, n);
-  const int out = ((m * n * F * 4) + 15) & ~15;
-  return F * (sh.a_bytes + sh.b_bytes) + tc::group_freqs(sh, F, bufcols) * sh.red_bytes + out;
+// Dynamic shared memory of one product's CTA with F frequencies staged: the
+// byte tiles of A' and B' and the results of the F frequencies.
+int tc_smem_bytes(int m, int k, int n, int F) {
+  const tc::Shape sh = tc::shape_of(m, k, n, F);
+  return (F / sh.phi) * (sh.a_bytes + sh.b_bytes) + ((m * n * (F + 1) * 4 + 15) & ~15);
 }
 
-// Accumulator buffer width, frequencies staged at once (F) and dynamic shared
-// memory of a launch over products of the given shapes.  The buffer is the
-// widest accumulator rounded up to a power of two (narrow products then
-// leave TMEM for a second CTA on the SM); F is the largest that lets as many
-// CTAs share an SM as TMEM allows (at most two), else the largest that fits.
+// Accumulator buffer width, frequencies staged at once (F), dynamic shared
+// memory and threads of a launch over products of the given shapes.  The
+// buffer is the widest accumulator rounded up to a power of two, at least
+// the floor below; CTAs share an SM as far as TMEM allows (four of 128
+// threads, two of 256, or one of 512), and F is the largest whose shared
+// memory lets them, else the launch takes fewer CTAs an SM.
 static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* F, int* smem,
-                             bool* wide) {
+                             int* threads) {
   int widest = 0;
   for (int i = 0; i < nshapes; ++i) {
-    const int c = tc::unit_cols(tc::shape_of(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]));
+    // the accumulator width does not depend on F
+    const int c =
+        tc::unit_cols(tc::shape_of(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], 1));
     if (c > widest) widest = c;
   }
-  int b = 32;
-  while (b < widest) b <<= 1;
-  // tuning: a wider buffer groups more frequencies of narrow products per
-  // commit at the cost of the second CTA on the SM (MPZMM_TC_BUFCOLS, a
-  // power of two up to 256)
-  static const int b_env = [] {
+  // The narrowest buffer is 64 columns, so four double-buffered CTAs of
+  // 128 threads share an SM and overlap one another's staging, MMA round
+  // trips and barriers: 4096 products of 2..16 rows and columns forced onto
+  // the tensor cores contracted in 74 ms that way, 107 ms with 128 columns
+  // (two CTAs of 256 threads an SM).  MPZMM_TC_BUFCOLS (a power of two from
+  // 32 to 256) replaces that floor for tuning.
+  static const int b_floor = [] {
     const char* e = std::getenv("MPZMM_TC_BUFCOLS");
     const int v = e ? std::atoi(e) : 0;
-    return (v >= 32 && v <= 256 && (v & (v - 1)) == 0) ? v : 0;
+    return (v >= 32 && v <= 256 && (v & (v - 1)) == 0) ? v : 64;
   }();
-  if (b_env > b) b = b_env;
+  int b = b_floor;
+  while (b < widest) b <<= 1;
   *bufcols = b;
   const int tcols = tc::double_buffered(b) ? 2 * b : b;
-  const int per_sm = 512 / tcols >= 2 ? 2 : 1;
-  for (int target = per_sm; target >= 1; --target) {
+  const int per_sm = 512 / tcols >= 4 ? 4 : (512 / tcols >= 2 ? 2 : 1);
+  for (int target = per_sm; target >= 1; target >>= 1) {
     const int limit = target == 1 ? tc::kDynSmemLimit
                                   : (tc::kSmemLimit / target) - tc::kStaticSmem - 1024;
     for (int f = 16; f >= 1; f >>= 1) {
       int bytes = 0;
       for (int i = 0; i < nshapes; ++i) {
-        const int sb = tc_smem_bytes(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], f, b);
+        const int sb = tc_smem_bytes(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2], f);
         if (sb > bytes) bytes = sb;
       }
-      // below four staged frequencies a second CTA is not worth the loss
+      // below four staged frequencies a shared SM is not worth the loss
       if (bytes <= limit && (target == 1 || f >= 4)) {
         *F = f;
         *smem = bytes;
-        *wide = target == 1;  // one CTA an SM: twice the threads
+        *threads = 512 / target;  // as many threads an SM either way
         return true;
       }
     }
@@ -2048,13 +2057,15 @@ static bool tc_launch_config(const int* shapes, int nshapes, int* bufcols, int* 
 }
 
 template <int F>
-static void launch_tc_f(int count, int smem, bool wide, cudaStream_t st, const ProdDesc* prods,
-                        const ContractItem* items, uint32_t* res, int bufcols, int* status,
-                        int stall) {
-  if (wide)
+static void launch_tc_f(int count, int smem, int threads, cudaStream_t st,
+                        const ProdDesc* prods, const ContractItem* items, uint32_t* res,
+                        int bufcols, int* status, int stall) {
+  if (threads == 512)
     k_contract_tc<F, 512><<<count, 512, smem, st>>>(prods, items, res, bufcols, status, stall);
-  else
+  else if (threads == 256)
     k_contract_tc<F, 256><<<count, 256, smem, st>>>(prods, items, res, bufcols, status, stall);
+  else
+    k_contract_tc<F, 128><<<count, 128, smem, st>>>(prods, items, res, bufcols, status, stall);
 }
 
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
@@ -2064,16 +2075,15 @@ cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items,
   for (int i = 0; i < nshapes; ++i)
     if (!contract_tc_eligible(shapes[3 * i], shapes[3 * i + 1], shapes[3 * i + 2]))
       return cudaErrorInvalidValue;
-  int F = 0, smem = 0, bufcols = 0;
-  bool wide = false;
-  if (!tc_launch_config(shapes, nshapes, &bufcols, &F, &smem, &wide))
+  int F = 0, smem = 0, bufcols = 0, threads = 0;
+  if (!tc_launch_config(shapes, nshapes, &bufcols, &F, &smem, &threads))
     return cudaErrorInvalidValue;
   switch (F) {
-    case 16: launch_tc_f<16>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
-    case 8: launch_tc_f<8>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
-    case 4: launch_tc_f<4>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
-    case 2: launch_tc_f<2>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
-    default: launch_tc_f<1>(count, smem, wide, st, prods, items, res, bufcols, status, stall); break;
+    case 16: launch_tc_f<16>(count, smem, threads, st, prods, items, res, bufcols, status, stall); break;
+    case 8: launch_tc_f<8>(count, smem, threads, st, prods, items, res, bufcols, status, stall); break;
+    case 4: launch_tc_f<4>(count, smem, threads, st, prods, items, res, bufcols, status, stall); break;
+    case 2: launch_tc_f<2>(count, smem, threads, st, prods, items, res, bufcols, status, stall); break;
+    default: launch_tc_f<1>(count, smem, threads, st, prods, items, res, bufcols, status, stall); break;
   }
   return cudaGetLastError();
 }
@@ -2214,10 +2224,11 @@ cudaError_t init_kernel_attributes() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)) !=
           cudaSuccess)
     return e;
-  for (auto fn : {k_contract_tc<16, 256>, k_contract_tc<8, 256>, k_contract_tc<4, 256>,
-                  k_contract_tc<2, 256>, k_contract_tc<1, 256>, k_contract_tc<16, 512>,
-                  k_contract_tc<8, 512>, k_contract_tc<4, 512>, k_contract_tc<2, 512>,
-                  k_contract_tc<1, 512>})
+  for (auto fn : {k_contract_tc<16, 128>, k_contract_tc<8, 128>, k_contract_tc<4, 128>,
+                  k_contract_tc<2, 128>, k_contract_tc<1, 128>, k_contract_tc<16, 256>,
+                  k_contract_tc<8, 256>, k_contract_tc<4, 256>, k_contract_tc<2, 256>,
+                  k_contract_tc<1, 256>, k_contract_tc<16, 512>, k_contract_tc<8, 512>,
+                  k_contract_tc<4, 512>, k_contract_tc<2, 512>, k_contract_tc<1, 512>})
     if ((e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   tc::kDynSmemLimit)) != cudaSuccess)
       return e;

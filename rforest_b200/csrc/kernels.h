@@ -71,7 +71,7 @@ cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_
 // wait runs out.
 bool contract_tc_eligible(int m, int k, int n);
 int contract_tc_freqs();
-int tc_smem_bytes(int m, int k, int n, int F, int bufcols);
+int tc_smem_bytes(int m, int k, int n, int F);
 cudaError_t launch_contract_tc(const ProdDesc* prods, const ContractItem* items, int count,
                                uint32_t* res, const int* shapes, int nshapes, int* status,
                                cudaStream_t st, int stall = 0);

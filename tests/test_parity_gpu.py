@@ -194,6 +194,23 @@ def test_tc_random_shapes(tensor_cores, seed):
         assert C.to_ints() == want, (m, k, n, bits)
 
 
+def test_tc_packed_slot_edges(tensor_cores):
+    """Shapes at the edges of frequency packing (two or four frequencies an
+    MMA for m <= 16 and n <= 32, K' slots of k rounded up to 8) and just
+    past them, with transforms shorter than a staged block."""
+    rng = random.Random(4242)
+    for m in (1, 8, 9, 16, 17):
+        for k in (1, 8, 9, 24, 33):
+            for n in (1, 32, 33):
+                bits = rng.choice([40, 700])
+                Ai = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(m * k)]
+                Bi = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(k * n)]
+                C = api.matmul(m, k, n, PK.from_ints(Ai), PK.from_ints(Bi))
+                want = [sum(Ai[i * k + l] * Bi[l * n + j] for l in range(k))
+                        for i in range(m) for j in range(n)]
+                assert C.to_ints() == want, (m, k, n, bits)
+
+
 def test_tc_config2_golden(tensor_cores):
     p = W.config2()
     assert PK.digest(api.matmul(8, 8, 8, p.A, p.B)) == G.digests()["config2"]["C"]
