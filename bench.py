@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["config3", "config2", "config4", "config1",
-                                           "config4_small"],
+                                           "config4_small", "config4_mid"],
                     default="config3")
     ap.add_argument("--count", type=int, default=4096, help="products per batch (config3)")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -86,6 +86,8 @@ def make_workload(name, replicate, count):
         return [W.config4(replicate)]
     if name == "config4_small":
         return [W.config4(replicate, bits=1 << 16)]
+    if name == "config4_mid":
+        return [W.config4(replicate, bits=1 << 18)]
     return [W.config1(replicate)]
 
 
@@ -103,6 +105,9 @@ def workload_config(name, count):
     if name == "config4_small":
         return {"workload": "single 64x64x64 exact matmul (profiling size)",
                 "products_per_step": 1, "bits": "2^16, unsigned", "seed": 4001}
+    if name == "config4_mid":
+        return {"workload": "single 64x64x64 exact matmul (profiling size, over a wave of CTAs)",
+                "products_per_step": 1, "bits": "2^18, unsigned", "seed": 4001}
     return {"workload": "single 4x4x4 exact matmul", "products_per_step": 1,
             "bits": "4096, signed", "seed": 1001}
 
