@@ -799,8 +799,14 @@ def serving_benchmark(api, args):
                 finished[i] = True
             th.join()
             span = (max(dones) - min(subs)) / 1e9
+            t_first = min(subs)
+            worst = sorted(range(R), key=lambda i: -lat[i])[:3]
             return {"offered": lam, "requests": R, "throughput": R / span,
-                    "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "unit": "requests/s",
+                    "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "max_ms": max(lat),
+                    "slowest": [{"request": i, "pool_entry": i % npool,
+                                 "submitted_s": (subs[i] - t_first) / 1e9,
+                                 "latency_ms": lat[i]} for i in worst],
+                    "unit": "requests/s",
                     "products_per_batch": R / max(1, srv.stats()["batches"] - b0)}
 
         runs = []

@@ -420,7 +420,25 @@ void Workspace::release_device() {
   device_bytes = 0;
 }
 
+int Workspace::ensure_side() {
+  if (fork_ev) return kOk;
+  for (int i = 0; i < kSideStreams; ++i) {
+    CU(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking), "cudaStreamCreate");
+    CU(cudaEventCreateWithFlags(&join_ev[i], cudaEventDisableTiming), "cudaEventCreate");
+  }
+  CU(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming), "cudaEventCreate");
+  return kOk;
+}
+
 void Workspace::release() {
+  for (int i = 0; i < kSideStreams; ++i) {
+    if (side[i]) cudaStreamDestroy(side[i]);
+    if (join_ev[i]) cudaEventDestroy(join_ev[i]);
+    side[i] = nullptr;
+    join_ev[i] = nullptr;
+  }
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  fork_ev = nullptr;
   release_device();
   for (void* p : retired_host) cudaFreeHost(p);
   retired_host.clear();
@@ -1049,6 +1067,8 @@ int Plan::execute(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
   if (!use_graph_ || timing_) return launch_all(st, timing_);
   if (!graph_exec_) {
+    const int e0 = ws_->ensure_side();  // no stream or event creation inside the capture
+    if (e0 != kOk) return e0;
     CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     const int rc = launch_all(st, false);
     cudaGraph_t g = nullptr;
@@ -1065,6 +1085,35 @@ int Plan::execute(cudaStream_t st) {
   return kOk;
 }
 
+// Launches the n independent launches of one stage, launch(i, stream),
+// round-robin over st and the workspace's side streams, forked from st and
+// joined back to it, so each launch's last wave overlaps the next one's
+// first.  MPZMM_FANOUT=0 keeps them all on st (tuning experiments).
+template <class L>
+static int fan_out(Workspace* ws, cudaStream_t st, int n, L launch) {
+  static const bool on = [] {
+    const char* e = std::getenv("MPZMM_FANOUT");
+    return !(e && e[0] == '0');
+  }();
+  int ns = n - 1 < Workspace::kSideStreams ? n - 1 : Workspace::kSideStreams;
+  if (!on || ns <= 0 || ws->ensure_side() != kOk) ns = 0;
+  if (ns > 0) {
+    CU(cudaEventRecord(ws->fork_ev, st), "cudaEventRecord");
+    for (int i = 0; i < ns; ++i)
+      CU(cudaStreamWaitEvent(ws->side[i], ws->fork_ev, 0), "cudaStreamWaitEvent");
+  }
+  for (int i = 0; i < n; ++i) {
+    const int w = ns > 0 ? i % (ns + 1) : 0;
+    const int r = launch(i, w == 0 ? st : ws->side[w - 1]);
+    if (r != kOk) return r;
+  }
+  for (int i = 0; i < ns; ++i) {
+    CU(cudaEventRecord(ws->join_ev[i], ws->side[i]), "cudaEventRecord");
+    CU(cudaStreamWaitEvent(st, ws->join_ev[i], 0), "cudaStreamWaitEvent");
+  }
+  return kOk;
+}
+
 int Plan::launch_all(cudaStream_t st, bool timed) {
   const Context& ctx = context();
   cudaEvent_t ev[kStages + 1] = {};
@@ -1075,20 +1124,23 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
     }
     CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
   }
-  for (const Group& g : fwd_groups_) {
+  int r = fan_out(ws_, st, (int)fwd_groups_.size(), [&](int i, cudaStream_t s) -> int {
+    const Group& g = fwd_groups_[i];
     if (g.large)
       CU(launch_large_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.lgN, g.D,
-                          ws_->d_limbs, ws_->d_res, ctx.d_twf, ctx.twist_f, st),
+                          ws_->d_limbs, ws_->d_res, ctx.d_twf, ctx.twist_f, s),
          "split+forward NTT launch (four-step)");
     else if (g.batched)
       CU(launch_fwd_items(d_fwd_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.D, g.team,
-                          g.max_lgN, ws_->d_limbs, ws_->d_res, ctx.d_twf, st, g.tiled),
+                          g.max_lgN, ws_->d_limbs, ws_->d_res, ctx.d_twf, s, g.tiled),
          "split+forward NTT launch");
     else
       CU(launch_split_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN,
-                          ws_->d_limbs, ws_->d_res, ctx.d_twf, st),
+                          ws_->d_limbs, ws_->d_res, ctx.d_twf, s),
          "split+forward NTT launch");
-  }
+    return kOk;
+  });
+  if (r != kOk) return r;
   if (timed) CU(cudaEventRecord(ev[1], st), "cudaEventRecord");
   if (!items_.empty())
     CU(launch_contract(d_pd_, d_items_, (int)items_.size(), ws_->d_res, st), "contraction launch");
@@ -1098,25 +1150,32 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
                           take_test_stall_tc() ? 1 : 0),
        "tensor-core contraction launch");
   if (timed) CU(cudaEventRecord(ev[2], st), "cudaEventRecord");
-  for (const Group& g : inv_groups_) {
+  r = fan_out(ws_, st, (int)inv_groups_.size(), [&](int i, cudaStream_t s) -> int {
+    const Group& g = inv_groups_[i];
     if (g.large)
       CU(launch_large_inv(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.lgN, ws_->d_res,
-                          ctx.d_twi, ctx.twist_i, st),
+                          ctx.d_twi, ctx.twist_i, s),
          "inverse NTT launch (four-step)");
     else if (g.batched)
       CU(launch_inv_items(d_inv_, d_idx_, d_cta_ + g.item_off, (int)g.items.size(), g.team,
-                          g.max_lgN, ws_->d_res, ctx.d_twi, st),
+                          g.max_lgN, ws_->d_res, ctx.d_twi, s),
          "inverse NTT launch");
     else
       CU(launch_inv_ntt(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.P, g.lgN, ws_->d_res,
-                        ctx.d_twi, st),
+                        ctx.d_twi, s),
          "inverse NTT launch");
-  }
+    return kOk;
+  });
+  if (r != kOk) return r;
   if (timed) CU(cudaEventRecord(ev[3], st), "cudaEventRecord");
-  for (const Group& g : rec_groups_)
+  r = fan_out(ws_, st, (int)rec_groups_.size(), [&](int i, cudaStream_t s) -> int {
+    const Group& g = rec_groups_[i];
     CU(launch_crt_mixed(d_inv_, d_idx_ + g.idx_off, (int)g.idx.size(), g.crt_high, g.rmin.data(),
-                        ws_->d_res, ws_->d_out, ws_->d_sizes, st),
+                        ws_->d_res, ws_->d_out, ws_->d_sizes, s),
        "CRT+recompose launch");
+    return kOk;
+  });
+  if (r != kOk) return r;
   if (timed) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
   return kOk;
 }

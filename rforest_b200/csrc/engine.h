@@ -102,6 +102,14 @@ struct Workspace {
   // device, which would stall every other batch in flight).
   bool retire_host = false;
   std::vector<void*> retired_host;
+  // Side streams a plan spreads one stage's independent launches over (so
+  // one launch's last wave overlaps the next launch's first), with the
+  // events that fork them off and join them back; created on first use.
+  static constexpr int kSideStreams = 2;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[kSideStreams] = {};
+  int ensure_side();
   // Ensures room for the given element counts (device buffers, then the
   // pinned staging of limbs and output words); returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,

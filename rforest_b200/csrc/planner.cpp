@@ -6,6 +6,9 @@
 // parameter choice is integer-only with an explicit exactness bound.
 #include "planner.h"
 
+#include <array>
+#include <cinttypes>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -261,6 +264,19 @@ bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* 
     const char* e = std::getenv("MPZMM_PMAX");
     return e ? std::atoi(e) : kMaxPrimes;
   }();
+  // cost-model weights: per point and stage of a transform, per point of a
+  // transform, per multiply-add of the contraction, per prime and per point
+  // of the CRT (MPZMM_COST="a,b,c,d,e" replaces them for tuning experiments)
+  static const std::array<int64_t, 5> wgt = [] {
+    std::array<int64_t, 5> w{5, 12, 2, 3, 10};
+    if (const char* e = std::getenv("MPZMM_COST")) {
+      std::array<int64_t, 5> v{};
+      if (std::sscanf(e, "%" SCNd64 ",%" SCNd64 ",%" SCNd64 ",%" SCNd64 ",%" SCNd64, &v[0], &v[1],
+                      &v[2], &v[3], &v[4]) == 5)
+        w = v;
+    }
+    return w;
+  }();
   const int64_t nfwd = (int64_t)m * k + (int64_t)k * n;
   const int64_t ninv = (int64_t)m * n;
   int64_t best = -1;
@@ -291,8 +307,8 @@ bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* 
     // per (prime, frequency) work: transforms, contraction, CRT/recompose
     const int64_t Nn = (int64_t)1 << lgN;
     const int64_t cost = P * Nn *
-                         ((nfwd + ninv) * (5 * lgN + 12) + 2 * (int64_t)m * n * k +
-                          ninv * (3 * P + 10));
+                         ((nfwd + ninv) * (wgt[0] * lgN + wgt[1]) + wgt[2] * (int64_t)m * n * k +
+                          ninv * (wgt[3] * P + wgt[4]));
     if (best < 0 || cost < best) {
       best = cost;
       out->P = P;
