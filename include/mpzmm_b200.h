@@ -318,8 +318,10 @@ MPZMM_API int mpzmm_plan_info(const mpzmm_plan *plan, int64_t *launches_per_exec
    8 MiB of static transform tables), held on every GPU that loads the
    library until exit; products needing more scratch, or a transform longer
    than 2^15 points, are rejected with MPZMM_ERR_TOO_LARGE.  The first call
-   on a device sets up that device's tables (make it before any stream
-   capture).  All calls share the one scratch array and leave their data in
+   on a device sets up that device's tables.  A call on a stream that is
+   capturing a CUDA graph is refused (MPZMM_ERR_ARG): its descriptors come
+   from a host buffer the next call overwrites, so a replay would be wrong.
+   All calls share the one scratch array and leave their data in
    it: calls whose GPU work overlaps race, so serialise them.  Nothing of
    the caller's is touched when a call is refused.  The kernels run
    asynchronously on `stream` (NULL: the legacy default stream); the call
@@ -335,8 +337,10 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
 
 /* ---- continuous-batching server (no counterpart in the reference) ----
    Up to `slots` batches are in flight, each slot with its own host thread,
-   CUDA stream and workspace.  Whenever a slot is free it admits queued
-   requests in arrival order into one batch while their estimated device
+   CUDA stream and workspace.  Whenever a slot is free it admits the oldest
+   queued request and then later ones of the same size class (small: at
+   most 16 MB of inputs and outputs; large: more), in arrival order, into
+   one batch while their estimated device
    footprint fits what the in-flight batches leave of `budget_bytes` (0:
    three quarters of the free device memory), with at most `max_batch`
    products per batch (0: no limit) and at most 256 MB of inputs and outputs
@@ -344,8 +348,12 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
    batches run join the next batch; a request's residues stay on the device
    for the whole pipeline.  Each slot's pinned staging is allocated once at
    creation and its device memory comes from a stream-ordered pool of the
-   server's own, so no batch synchronises the device.  A request larger than
-   the budget is refused (MPZMM_ERR_TOO_LARGE). */
+   server's own, so no batch synchronises the device.  Each slot has two
+   streams: batches of small requests run on one of the device's greatest
+   stream priority, batches of large ones on one of its least, so a small
+   request waits neither inside a large one's batch nor behind its queued
+   GPU work.  A request larger than the budget is refused
+   (MPZMM_ERR_TOO_LARGE). */
 typedef struct mpzmm_server mpzmm_server;
 MPZMM_API int mpzmm_server_create(mpzmm_server **server, int64_t budget_bytes, int slots,
                                   int max_batch);

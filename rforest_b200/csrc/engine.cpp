@@ -575,7 +575,12 @@ static int plan_product(const ProductSpec& ps, Params* prm, std::string* msg) {
 }
 
 int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
-  if (built_) return set_error(kErrState, "plan already built");
+  const int r = prepare(std::move(prods));
+  return r ? r : bind(ws);
+}
+
+int Plan::prepare(std::vector<ProductSpec> prods) {
+  if (built_ || prepared_) return set_error(kErrState, "plan already built");
   prods_ = std::move(prods);
   const int block_freqs = contract_block_freqs();
   params_.resize(prods_.size());
@@ -877,7 +882,12 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
       g.idx_off = (uint32_t)idx_all_.size();
       idx_all_.insert(idx_all_.end(), g.idx.begin(), g.idx.end());
     }
+  prepared_ = true;
+  return kOk;
+}
 
+int Plan::bind(Workspace* ws) {
+  if (!prepared_ || built_) return set_error(kErrState, "plan not prepared, or already bound");
   // device and pinned buffers
   Context& ctx = context();
   if (!ctx.ready) return set_error(kErrState, "not set up (call hw_mpz_setup)");
@@ -1067,8 +1077,10 @@ int Plan::execute(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
   if (!use_graph_ || timing_) return launch_all(st, timing_);
   if (!graph_exec_) {
-    const int e0 = ws_->ensure_side();  // no stream or event creation inside the capture
-    if (e0 != kOk) return e0;
+    if (ws_->fanout) {  // no stream or event creation inside the capture
+      const int e0 = ws_->ensure_side();
+      if (e0 != kOk) return e0;
+    }
     CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     const int rc = launch_all(st, false);
     cudaGraph_t g = nullptr;
@@ -1088,7 +1100,9 @@ int Plan::execute(cudaStream_t st) {
 // Launches the n independent launches of one stage, launch(i, stream),
 // round-robin over st and the workspace's side streams, forked from st and
 // joined back to it, so each launch's last wave overlaps the next one's
-// first.  MPZMM_FANOUT=0 keeps them all on st (tuning experiments).
+// first.  MPZMM_FANOUT=0 keeps them all on st (tuning experiments), and so
+// does a workspace with fanout off (the server's: each of its batches keeps
+// the priority of its own stream).
 template <class L>
 static int fan_out(Workspace* ws, cudaStream_t st, int n, L launch) {
   static const bool on = [] {
@@ -1096,7 +1110,7 @@ static int fan_out(Workspace* ws, cudaStream_t st, int n, L launch) {
     return !(e && e[0] == '0');
   }();
   int ns = n - 1 < Workspace::kSideStreams ? n - 1 : Workspace::kSideStreams;
-  if (!on || ns <= 0 || ws->ensure_side() != kOk) ns = 0;
+  if (!on || !ws->fanout || ns <= 0 || ws->ensure_side() != kOk) ns = 0;
   if (ns > 0) {
     CU(cudaEventRecord(ws->fork_ev, st), "cudaEventRecord");
     for (int i = 0; i < ns; ++i)
@@ -1316,6 +1330,15 @@ uint64_t input_limbs(const ProductSpec& ps) {
   return n;
 }
 
+int pipe_depth() {
+  static const int d = [] {
+    const char* e = std::getenv("MPZMM_PIPE_DEPTH");
+    const int v = e ? std::atoi(e) : 0;
+    return v >= 2 && v <= kPipeDepth ? v : 4;
+  }();
+  return d;
+}
+
 int ensure_pipeline(Context& ctx) {
   while ((int)ctx.pipe_ws.size() < kPipeDepth)
     ctx.pipe_ws.push_back(ctx.pipe_ws.empty() ? ctx.ws : new Workspace);
@@ -1486,6 +1509,7 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
   // The caller's thread plans chunks and waits for finished ones; a
   // submitter thread queues each chunk's copies and kernels, because queueing
   // a copy can block the host until the copy engine takes it.
+  const int depth = pipe_depth();
   std::unique_ptr<Plan> plans[kPipeDepth];
   size_t slot_chunk[kPipeDepth] = {};
   bool slot_ok[kPipeDepth] = {};
@@ -1508,7 +1532,7 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
         c = queue.front();
         queue.pop_front();
       }
-      const int w = (int)(c % kPipeDepth);
+      const int w = (int)(c % depth);
       Plan* p = plans[w].get();
       cudaStream_t ps = ctx.pipe_st[w];
       const int64_t t0 = now_ns();
@@ -1573,23 +1597,29 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     plans[w].reset();
   };
   for (size_t c = 0; c < nchunks; ++c) {
-    const int w = (int)(c % kPipeDepth);
-    finish(w);  // the chunk that last used this workspace
-    if (stop) break;
+    const int w = (int)(c % depth);
+    // the chunk is planned before waiting for the workspace it will use, so
+    // the wait (for the results of the chunk `depth` back) and the planning
+    // overlap, and the chunk is queued as soon as the workspace is free
     std::vector<ProductSpec> part;
     part.reserve(bounds[c + 1] - bounds[c]);
     for (size_t t = bounds[c]; t < bounds[c + 1]; ++t) part.push_back(std::move(specs[t]));
-    plans[w].reset(new Plan);
+    std::unique_ptr<Plan> np(new Plan);
     const int64_t t0 = now_ns();
-    const int r = plans[w]->build(std::move(part), ctx.pipe_ws[w]);
+    int r = np->prepare(std::move(part));
+    const int64_t tp = now_ns();
+    finish(w);  // the chunk that last used this workspace
+    if (stop) break;
+    const int64_t tb = now_ns();
+    if (!r) r = np->bind(ctx.pipe_ws[w]);
     const int64_t t1 = now_ns();
-    ctx.batch_ns[0] += t1 - t0;
+    ctx.batch_ns[0] += (tp - t0) + (t1 - tb);
     if (r) {
       if (!status) status = r;
       stop = true;
-      plans[w].reset();
       break;
     }
+    plans[w] = std::move(np);
     count_bytes(*plans[w]);
     double* row = tl + c * kTimelineFields;
     row[0] = (t0 - tl0) * 1e-6;
@@ -1602,8 +1632,8 @@ int run_batch(std::vector<ProductSpec> specs, cudaStream_t st) {
     cv.notify_all();
   }
   // drain in chunk order (every chunk in flight is waited for, also on error)
-  for (size_t c = nchunks > (size_t)kPipeDepth ? nchunks - kPipeDepth : 0; c < nchunks; ++c)
-    finish((int)(c % kPipeDepth));
+  for (size_t c = nchunks > (size_t)depth ? nchunks - depth : 0; c < nchunks; ++c)
+    finish((int)(c % depth));
   {
     std::lock_guard<std::mutex> lk(mu);
     closing = true;

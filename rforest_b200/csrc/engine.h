@@ -106,6 +106,7 @@ struct Workspace {
   // one launch's last wave overlaps the next launch's first), with the
   // events that fork them off and join them back; created on first use.
   static constexpr int kSideStreams = 2;
+  bool fanout = true;  // false: every launch on the plan's own stream
   cudaStream_t side[kSideStreams] = {};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[kSideStreams] = {};
@@ -181,8 +182,9 @@ struct Context {
 // ms), bytes in, bytes out.
 constexpr int kTimelineFields = 10;
 
-// Chunks in flight in a pipelined one-shot batch.
-constexpr int kPipeDepth = 4;
+// Workspaces a pipelined one-shot batch may cycle through (chunks in
+// flight); it uses MPZMM_PIPE_DEPTH of them, 2 .. kPipeDepth, default 4.
+constexpr int kPipeDepth = 8;
 // Largest host gap (limbs) between consecutive entries in one pinned range
 // that a copy run bridges instead of starting a new copy.
 constexpr int64_t kRunGapLimbs = 256;
@@ -242,8 +244,16 @@ class Plan {
   static constexpr int kStages = 4;
   ~Plan();
   // Computes parameters, descriptors and launch groups, and reserves device
-  // and pinned host buffers in `ws` (the plan's own workspace if null).
+  // and pinned host buffers in `ws` (the plan's own workspace if null):
+  // prepare() then bind().
   int build(std::vector<ProductSpec> prods, Workspace* ws = nullptr);
+  // The host half of build(): parameters, descriptors, launch groups and
+  // transfer runs; touches no workspace, so a pipeline can plan a chunk
+  // while the workspace it will use is still busy with an earlier one.
+  int prepare(std::vector<ProductSpec> prods);
+  // The rest: reserves buffers in `ws` and writes the descriptors into its
+  // pinned staging.
+  int bind(Workspace* ws);
   // Copies the input limbs (and the descriptors) to the device: straight
   // from the caller's memory where it is pinned memory known to the library,
   // through the pinned staging buffer otherwise.
@@ -365,6 +375,7 @@ class Plan {
   size_t off_tc_ = 0;
   uint32_t* d_idx_ = nullptr;
   bool built_ = false;
+  bool prepared_ = false;
   bool timing_ = false;
   std::vector<cudaEvent_t> events_;  // kStages + 1 per timed execute
   bool use_graph_ = false;

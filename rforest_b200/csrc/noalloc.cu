@@ -110,13 +110,21 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   // the product descriptor holds the dimensions in 16 bits
   if (m > 65535 || k > 65535 || n > 65535)
     return set_error(kErrTooLarge, "mpzmm_matmul_noalloc: dimension > 65535");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the descriptors go up from one pageable host buffer that the next call
+  // overwrites, so a call captured into a CUDA graph would replay stale ones
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return cufail(e, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_error(kErrArg, "mpzmm_matmul_noalloc: the stream is capturing (calls cannot be "
+                              "captured into a CUDA graph)");
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cufail(e, "cudaGetDevice");
   DeviceState* ds = nullptr;
   int st = setup_device(dev, &ds);
   if (st) return st;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   // operand bit lengths bounded from the limb counts (the limbs are on the device)
   int64_t a_bits = 0, b_bits = 0;

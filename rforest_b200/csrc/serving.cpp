@@ -45,7 +45,8 @@ struct Ticket {
 };
 
 struct Slot {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;     // least priority: batches with much data
+  cudaStream_t stream_hi = nullptr;  // greatest priority: small batches
   Workspace ws;
   std::thread thread;
   bool busy = false;
@@ -64,6 +65,12 @@ struct mpzmm_server {
   // larger request goes alone), and every slot's pinned staging is sized to
   // it once, so batches never allocate pinned memory
   int64_t batch_host_cap = (int64_t)256 << 20;
+  // requests with at most this many host bytes are small: admission keeps
+  // them in batches of their own, which run on their slot's
+  // greatest-priority stream, so the block scheduler starts their CTAs ahead
+  // of those of large batches already on the GPU and a small request is
+  // held up neither inside nor behind a large one's batch (0: one class)
+  int64_t small_batch_bytes = (int64_t)16 << 20;
   // device memory of the slots' workspaces: a stream-ordered pool of the
   // server's own that keeps freed memory, so a workspace growing or being
   // released never synchronises the device or stalls the other slots
@@ -89,16 +96,30 @@ struct mpzmm_server {
     t->t_done = now_ns();
   }
 
-  // Admits queued requests for a free slot (lock held): FIFO, at most
-  // max_batch, while the estimated footprint fits the free budget; a
-  // request larger than the free budget runs once the GPU is otherwise idle.
+  // A request with at most small_batch_bytes of host data (0: none is).
+  bool is_small(const Ticket& t) const {
+    return small_batch_bytes > 0 && t.host_bytes <= small_batch_bytes;
+  }
+
+  // Admits queued requests for a free slot (lock held): the oldest request
+  // first, then later ones of the same size class (small or large) in
+  // arrival order, passing over the other class, which stays queued for
+  // another slot -- so small requests never wait inside a batch for a large
+  // one; at most max_batch, while the estimated footprint fits the free
+  // budget; a request larger than the free budget runs once the GPU is
+  // otherwise idle.
   void admit(std::vector<std::shared_ptr<Ticket>>& batch, int64_t& bytes) {
     int busy_slots = 0;
     for (auto& o : slots) busy_slots += o->busy ? 1 : 0;
     int64_t host = 0;
     for (const auto& t : batch) host += t->host_bytes;
-    while (!queue.empty() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
-      const auto& t = queue.front();
+    auto it = queue.begin();
+    while (it != queue.end() && (max_batch <= 0 || (int)batch.size() < max_batch)) {
+      const auto& t = *it;
+      if (!batch.empty() && is_small(*t) != is_small(*batch.front())) {
+        ++it;
+        continue;
+      }
       if (!batch.empty() && host + t->host_bytes > batch_host_cap) break;
       const bool fits = in_flight_bytes + bytes + t->bytes <= budget;
       const bool alone = batch.empty() && busy_slots == 0 && in_flight_bytes == 0 &&
@@ -107,7 +128,7 @@ struct mpzmm_server {
       bytes += t->bytes;
       host += t->host_bytes;
       batch.push_back(t);
-      queue.pop_front();
+      it = queue.erase(it);
       if (!fits) break;
     }
   }
@@ -117,23 +138,30 @@ struct mpzmm_server {
     std::vector<ProductSpec> specs;
     specs.reserve(batch.size());
     for (auto& t : batch) specs.push_back(t->spec);
+    // a batch of small requests (admission keeps the classes apart) runs on
+    // the greatest-priority stream.  The slot's batches run one after
+    // another, each ending with a stream synchronisation, so switching
+    // streams between batches needs no event; the workspace's stream-ordered
+    // allocations follow the batch's stream.
+    const cudaStream_t bs = is_small(*batch.front()) ? s.stream_hi : s.stream;
+    s.ws.async_stream = bs;
     Plan plan;
     const int64_t a0 = now_ns();
     int st = plan.build(std::move(specs), &s.ws);
     const int64_t a1 = now_ns();
-    if (!st) st = plan.upload(s.stream);
+    if (!st) st = plan.upload(bs);
     const int64_t a2 = now_ns();
-    if (!st) st = plan.execute(s.stream);
+    if (!st) st = plan.execute(bs);
     const int64_t a3 = now_ns();
     {
       std::lock_guard<std::mutex> lk(mu);
       for (auto& t : batch) t->t_start = a3;
     }
-    if (!st) st = plan.download(s.stream);
+    if (!st) st = plan.download(bs);
     const int64_t a4 = now_ns();
     if (st) {
       *err = last_error();
-      cudaStreamSynchronize(s.stream);  // whatever was queued
+      cudaStreamSynchronize(bs);  // whatever was queued
     }
     std::lock_guard<std::mutex> lk(mu);
     ns_build += a1 - a0;
@@ -237,17 +265,34 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
                                      cudaGetErrorString(e));
     }
   }
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+    cudaGetLastError();
+    least = greatest = 0;
+  }
+  static const bool prio_on = [] {
+    const char* e = std::getenv("MPZMM_SERVER_PRIORITY");
+    return !(e && e[0] == '0');
+  }();
+  if (!prio_on) s->small_batch_bytes = 0;
   for (int i = 0; i < slots; ++i) {
     std::unique_ptr<Slot> sl(new Slot);
-    cudaError_t e = cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithPriority(&sl->stream, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess)
+      e = cudaStreamCreateWithPriority(&sl->stream_hi, cudaStreamNonBlocking, greatest);
     if (e != cudaSuccess) {
-      for (auto& o : s->slots) cudaStreamDestroy(o->stream);
+      if (sl->stream) cudaStreamDestroy(sl->stream);
+      for (auto& o : s->slots) {
+        cudaStreamDestroy(o->stream);
+        cudaStreamDestroy(o->stream_hi);
+      }
       cudaMemPoolDestroy(s->pool);
       return set_error(kErrCuda, cudaGetErrorString(e));
     }
     sl->ws.async_stream = sl->stream;
     sl->ws.pool = s->pool;
     sl->ws.retire_host = true;
+    sl->ws.fanout = false;  // one stream a batch: its priority holds for every launch
     s->slots.push_back(std::move(sl));
   }
   mpzmm_server* raw = s.get();
@@ -382,9 +427,12 @@ void mpzmm_server_destroy(mpzmm_server* s) {
     if (sl->thread.joinable()) sl->thread.join();
   for (auto& sl : s->slots) {
     cudaStreamSynchronize(sl->stream);
-    sl->ws.release();  // stream-ordered frees on the slot's stream
+    cudaStreamSynchronize(sl->stream_hi);
+    sl->ws.release();  // stream-ordered frees on the last batch's stream
     cudaStreamSynchronize(sl->stream);
+    cudaStreamSynchronize(sl->stream_hi);
     cudaStreamDestroy(sl->stream);
+    cudaStreamDestroy(sl->stream_hi);
   }
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;

@@ -79,9 +79,10 @@ def test_noalloc_rejects_oversize(product_lib):
     assert "scratch" in str(e.value) or "limit" in str(e.value)
 
 
-def _noalloc_raw(m, k, n, A: PK.Packed, B: PK.Packed, cap_delta=0):
+def _noalloc_raw(m, k, n, A: PK.Packed, B: PK.Packed, cap_delta=0, capture=False):
     """One call with explicit capacities (the bound plus cap_delta); returns
-    (status, result sizes on the device after the call)."""
+    (status, result sizes on the device after the call).  capture: the call
+    is made on a side stream while it captures a CUDA graph."""
     import torch
     L = _lib.lib()
     cap = api.output_limbs(k, 64 * A.max_limbs(), 64 * B.max_limbs()) + cap_delta
@@ -96,14 +97,23 @@ def _noalloc_raw(m, k, n, A: PK.Packed, B: PK.Packed, cap_delta=0):
     a_sz = np.ascontiguousarray(A.sizes, dtype=np.int32)
     b_offs = np.ascontiguousarray(B.offs, dtype=np.int64)
     b_sz = np.ascontiguousarray(B.sizes, dtype=np.int32)
-    stream = torch.cuda.current_stream(dev)
-    st = L.mpzmm_matmul_noalloc(
-        m, k, n, C.c_void_p(d_a.data_ptr()), a_offs.ctypes.data_as(_lib.i64p),
-        a_sz.ctypes.data_as(_lib.i32p), C.c_void_p(d_b.data_ptr()),
-        b_offs.ctypes.data_as(_lib.i64p), b_sz.ctypes.data_as(_lib.i32p),
-        C.c_void_p(d_c.data_ptr()), c_offs.ctypes.data_as(_lib.i64p),
-        c_caps.ctypes.data_as(_lib.i64p), C.c_void_p(d_sz.data_ptr()),
-        C.c_void_p(stream.cuda_stream))
+    def call(stream):
+        return L.mpzmm_matmul_noalloc(
+            m, k, n, C.c_void_p(d_a.data_ptr()), a_offs.ctypes.data_as(_lib.i64p),
+            a_sz.ctypes.data_as(_lib.i32p), C.c_void_p(d_b.data_ptr()),
+            b_offs.ctypes.data_as(_lib.i64p), b_sz.ctypes.data_as(_lib.i32p),
+            C.c_void_p(d_c.data_ptr()), c_offs.ctypes.data_as(_lib.i64p),
+            c_caps.ctypes.data_as(_lib.i64p), C.c_void_p(d_sz.data_ptr()),
+            C.c_void_p(stream.cuda_stream))
+
+    if capture:
+        side = torch.cuda.Stream(dev)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side, capture_error_mode="relaxed"):
+            st = call(side)
+        del graph
+    else:
+        st = call(torch.cuda.current_stream(dev))
     torch.cuda.synchronize(dev)
     return st, d_sz.cpu().numpy().tolist()
 
@@ -131,3 +141,19 @@ def test_noalloc_rejects_short_capacity_untouched(product_lib):
     st, sizes = _noalloc_raw(2, 2, 2, A, B)
     assert st == _lib.MPZMM_OK
     assert sizes != [777] * 4
+
+
+def test_noalloc_refuses_a_capturing_stream(product_lib):
+    """Its descriptors come from a host buffer the next call overwrites, so a
+    call captured into a CUDA graph would replay stale ones: refused with
+    MPZMM_ERR_ARG while the stream captures, nothing touched; the same call
+    outside the capture succeeds."""
+    A = PK.from_ints([(1 << 300) + 9, -17])
+    B = PK.from_ints([5, (1 << 200) - 1])
+    st, sizes = _noalloc_raw(1, 2, 1, A, B, capture=True)
+    assert st == _lib.MPZMM_ERR_ARG
+    assert "captur" in _lib.lib().mpzmm_last_error().decode()
+    assert sizes == [777]
+    st, sizes = _noalloc_raw(1, 2, 1, A, B)
+    assert st == _lib.MPZMM_OK
+    assert sizes != [777]
