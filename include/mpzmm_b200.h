@@ -104,7 +104,7 @@ MPZMM_API int mpzmm_setup(int device);
 /* Options (process-wide; a plan keeps the values it was built with).
    MPZMM_OPT_CONTRACT selects the frequency-domain contraction engine:
    0 automatic (per size class, the engine mpzmm_autotune measured faster;
-   tensor cores -- tcgen05 kind::i8 -- only for m <= 128, k <= 64, n <= 64),
+   tensor cores -- tcgen05 kind::i8 -- only for m, n <= 1024 and k <= 64),
    1 CUDA cores only, 2 tensor cores wherever the shape allows.
    The environment variable MPZMM_CONTRACT sets the initial value.
    MPZMM_OPT_CHUNK_LIMBS sets the input limbs per chunk of a pipelined
@@ -164,13 +164,15 @@ MPZMM_API int mpzmm_batch_timeline(double *rows, int max_chunks, int *nchunks);
 MPZMM_API int mpzmm_batch_chunks(int count, const int64_t *limbs, int64_t chunk_limbs,
                                  int64_t *bounds, int max_bounds, int *nchunks);
 
-/* Autotuner: times the contraction of a representative batch per size
-   class (m = n = 4, 8, 16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit
-   entries, copies of one product until every SM has several blocks' work)
-   on CUDA cores and on tensor cores and makes automatic mode use tensor
-   cores for that class where they took under 3/4 of the CUDA-core time
-   (until then automatic mode uses CUDA cores).  ms_out, if not NULL, receives 40 floats: {CUDA, tensor}
-   milliseconds per class, k-major. */
+/* Autotuner: times a representative batch per size class (m = n = 4, 8,
+   16, 32, 64 by k = 8, 16, 32, 64 terms, 2^14-bit entries, copies of one
+   product until every SM has several blocks' work) on CUDA cores and on
+   tensor cores and makes automatic mode use tensor cores for that class
+   where their split + forward + contraction took under 9/10 of the
+   CUDA-core time (their operands are written frequency-blocked, which
+   costs the forward a little; until the autotuner runs automatic mode uses
+   CUDA cores).  ms_out, if not NULL, receives 40 floats: {CUDA, tensor}
+   contraction milliseconds per class, k-major. */
 MPZMM_API int mpzmm_autotune(void *stream, float *ms_out);
 
 /* Human-readable message for the last error on the calling thread. */

@@ -175,7 +175,7 @@ int mpzmm_autotune(void* stream, float* ms_out) {
       int64_t copies = (8 * (int64_t)context().num_sms + ctas - 1) / (ctas > 0 ? ctas : 1);
       if (copies < 1) copies = 1;
       if (copies > 256) copies = 256;
-      float ms[2] = {0.f, 0.f};
+      float ms[2] = {0.f, 0.f}, fc[2] = {0.f, 0.f};  // contraction; split + forward + contraction
       for (int mode = 1; mode <= 2; ++mode) {
         std::vector<ProductSpec> v;
         for (int64_t c = 0; c < copies; ++c) {
@@ -197,19 +197,23 @@ int mpzmm_autotune(void* stream, float* ms_out) {
         // fastest of five timed executes: one slow repeat (another process
         // on the device, a clock change) must not decide the table
         plan.set_timing(true);
-        float best = -1.f;
+        float best = -1.f, best_fc = -1.f;
         for (int rep = 0; rep < 5; ++rep) {
           if ((st = plan.execute(s))) return fail(st);
           float t[Plan::kStages];
           int64_t ex = 0;  // stage_times returns (and clears) this execute's times
           if ((st = plan.stage_times(t, &ex))) return fail(st);
           if (best < 0.f || t[1] < best) best = t[1];
+          if (best_fc < 0.f || t[0] + t[1] < best_fc) best_fc = t[0] + t[1];
         }
         ms[mode - 1] = best < 0.f ? 0.f : best;
+        fc[mode - 1] = best_fc < 0.f ? 0.f : best_fc;
       }
-      // tensor cores only with a clear margin (a near tie measured on a
-      // probe once turned into a far slower contraction of a real batch)
-      context().tc_pref[bk][bm] = ms[1] < 0.75f * ms[0] ? 1 : 0;
+      // the decision weighs split + forward with the contraction (tensor-core
+      // operands are written frequency-blocked, which costs the forward a
+      // little), and wants a 10 % margin (a near tie measured on a probe once
+      // turned into a far slower contraction of a real batch)
+      context().tc_pref[bk][bm] = fc[1] < 0.9f * fc[0] ? 1 : 0;
       if (ms_out) {
         ms_out[2 * (bk * 5 + bm)] = ms[0];
         ms_out[2 * (bk * 5 + bm) + 1] = ms[1];

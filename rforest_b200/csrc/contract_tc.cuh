@@ -20,7 +20,8 @@
 // into one MMA (Shape).
 //
 // One CTA of 128, 256 or 512 threads (four, two or one an SM, as TMEM and
-// shared memory allow) per (product, prime, block of 128 frequencies),
+// shared memory allow) per (product, prime, block of 128 frequencies, block
+// of at most 32 rows and 32 columns of C: its rows of A and columns of B),
 // processed F frequencies at a time: all warps stage A' and B' of the F
 // frequencies straight from global memory (F consecutive residues of a
 // polynomial per vector load) into canonical K-major no-swizzle tiles (8-row
@@ -44,8 +45,9 @@ namespace mpzmm {
 namespace tc {
 
 constexpr int kMaxK = 64;        // k <= 64: K' = k bytes padded to 32, z < 2^57
-constexpr int kMaxN = 64;        // n <= 64: at most two units of 32 outputs a frequency
-constexpr int kMaxM = 128;       // m <= 128: four planes in four 128-lane tiles
+constexpr int kBlock = kTcBlock;  // rows i and columns l of C a work item covers
+constexpr int kMaxN = 1024;      // n, m <= 1024: block indices fit the item's 8-bit fields
+constexpr int kMaxM = 1024;
 constexpr int kFreqs = 128;      // frequencies per CTA (each polynomial's 512 bytes)
 constexpr int kUnitCols = 32;    // output columns l per unit
 constexpr uint32_t kSpinLimit = 1u << 26;

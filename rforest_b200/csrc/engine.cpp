@@ -748,22 +748,33 @@ int Plan::prepare(std::vector<ProductSpec> prods) {
     }
     const uint32_t prod_index = (uint32_t)pd_.size();
     pd_.push_back(pd);
-    if (use_tc) {
-      bool seen = false;
-      for (size_t q = 0; q < tc_shapes_.size() && !seen; q += 3)
-        seen = tc_shapes_[q] == m && tc_shapes_[q + 1] == k && tc_shapes_[q + 2] == n;
-      if (!seen) tc_shapes_.insert(tc_shapes_.end(), {m, k, n});
-    }
+    // tensor-core items cover blocks of at most kTcBlock rows and columns
+    // of C (the launch is sized for the blocks' shapes); CUDA-core items
+    // cover all of C
+    const int rbs = use_tc ? (m + kTcBlock - 1) / kTcBlock : 1;
+    const int cbs = use_tc ? (n + kTcBlock - 1) / kTcBlock : 1;
+    if (use_tc)
+      for (int rb = 0; rb < rbs; ++rb)
+        for (int cb = 0; cb < cbs; ++cb) {
+          const int bm = std::min(kTcBlock, m - rb * kTcBlock);
+          const int bn = std::min(kTcBlock, n - cb * kTcBlock);
+          bool seen = false;
+          for (size_t q = 0; q < tc_shapes_.size() && !seen; q += 3)
+            seen = tc_shapes_[q] == bm && tc_shapes_[q + 1] == k && tc_shapes_[q + 2] == bn;
+          if (!seen) tc_shapes_.insert(tc_shapes_.end(), {bm, k, bn});
+        }
     const uint64_t fstep = use_tc ? (uint64_t)kTcFreqsPerCta : (uint64_t)block_freqs;
     for (int j = 0; j < P; ++j)
-      for (uint64_t h0 = 0; h0 < N; h0 += fstep) {
-        ContractItem it;
-        it.prod = prod_index;
-        it.prime = (uint16_t)j;
-        it.pad = 0;
-        it.h0 = (uint32_t)h0;
-        (use_tc ? tc_items_ : items_).push_back(it);
-      }
+      for (uint64_t h0 = 0; h0 < N; h0 += fstep)
+        for (int rb = 0; rb < rbs; ++rb)
+          for (int cb = 0; cb < cbs; ++cb) {
+            ContractItem it;
+            it.prod = prod_index;
+            it.prime = (uint16_t)j;
+            it.pad = (uint16_t)((rb << 8) | cb);  // block of C (tensor cores only)
+            it.h0 = (uint32_t)h0;
+            (use_tc ? tc_items_ : items_).push_back(it);
+          }
     const uint64_t ncoef_c = (uint64_t)(prm.lenA + prm.lenB - 1);
     Group& ig = invg[{lgN, P}];
     ig.P = P;

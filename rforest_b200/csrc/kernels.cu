@@ -1383,7 +1383,12 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
   const int lane = tid & 31;
   const ContractItem it = items[blockIdx.x];
   const ProdDesc d = prods[it.prod];
-  const int m = d.m, k = d.k, n = d.n;
+  // the item's block of C: rows i_base .. + m, columns l_base .. + n (at
+  // most kBlock each); m, n below are the block's, d.m, d.n the product's
+  const int i_base = (int)(it.pad >> 8) * tc::kBlock, l_base = (int)(it.pad & 0xffu) * tc::kBlock;
+  const int m = d.m - i_base < tc::kBlock ? d.m - i_base : tc::kBlock;
+  const int n = d.n - l_base < tc::kBlock ? d.n - l_base : tc::kBlock;
+  const int k = d.k;
   const int N = 1 << d.lgN;
   const int j = it.prime;
   const uint32_t p = c_primes[j].p;
@@ -1485,9 +1490,11 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
           const int kk = kk0 + c;
           const bool ok = live && kk < k && r < (isA ? m : n);
           const uint64_t poly =
-              ok ? (isA ? (uint64_t)(r * k + kk) : (uint64_t)(kk * n + r)) : 0;
-          load_freqs<F>(res + (isA ? d.a_res : d.b_res), isA ? (uint64_t)m * k : (uint64_t)k * n,
-                        poly, tile0, sub0, ok, nf, x[w2][c]);
+              ok ? (isA ? (uint64_t)((i_base + r) * k + kk) : (uint64_t)(kk * d.n + l_base + r))
+                 : 0;
+          load_freqs<F>(res + (isA ? d.a_res : d.b_res),
+                        isA ? (uint64_t)d.m * k : (uint64_t)k * d.n, poly, tile0, sub0, ok, nf,
+                        x[w2][c]);
         }
       }
 #pragma unroll
@@ -1635,7 +1642,9 @@ k_contract_tc(const ProdDesc* __restrict__ prods, const ContractItem* __restrict
     // The next block's staging may start at once: this block's MMAs have
     // all completed, and its epilogue writes outs only after its own barrier.
     for (int e = tid; e < m * n; e += NT) {
-      uint32_t* dst = res + d.c_res + (uint64_t)e * stride + base;
+      const int ei = e / n, el = e - ei * n;  // the block's row and column
+      const uint64_t ge = (uint64_t)(i_base + ei) * (uint64_t)d.n + (uint64_t)(l_base + el);
+      uint32_t* dst = res + d.c_res + ge * stride + base;
       const uint32_t* sv = outs + e * (F + 1);
       if (nf == F && F >= 4) {
 #pragma unroll

@@ -89,6 +89,7 @@ struct FwdDesc {
   uint32_t tile_e = 0;
 };
 constexpr int kTcTile = 8;      // frequencies a block of the tensor-core layout (32 bytes)
+constexpr int kTcBlock = 32;    // rows and columns of C a tensor-core work item covers
 constexpr int kTcTileLg = 3;
 
 // One output polynomial of the inverse transform + CRT + recompose.
@@ -118,7 +119,7 @@ struct ProdDesc {
 struct ContractItem {
   uint32_t prod;
   uint16_t prime;
-  uint16_t pad;
+  uint16_t pad;        // tensor cores: block of C, (row block << 8) | column block
   uint32_t h0;         // first frequency of the block
 };
 

@@ -211,6 +211,20 @@ def test_tc_packed_slot_edges(tensor_cores):
                 assert C.to_ints() == want, (m, k, n, bits)
 
 
+def test_tc_row_column_blocks(tensor_cores):
+    """Products wider than one 32-row by 32-column block of C: each work
+    item covers one block (partial blocks at the edges)."""
+    rng = random.Random(777)
+    for (m, k, n) in [(33, 3, 1), (1, 64, 65), (64, 64, 64), (100, 20, 70), (200, 9, 33)]:
+        bits = rng.choice([50, 600])
+        Ai = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(m * k)]
+        Bi = [rng.randrange(-(1 << bits), 1 << bits) for _ in range(k * n)]
+        C = api.matmul(m, k, n, PK.from_ints(Ai), PK.from_ints(Bi))
+        want = [sum(Ai[i * k + l] * Bi[l * n + j] for l in range(k))
+                for i in range(m) for j in range(n)]
+        assert C.to_ints() == want, (m, k, n, bits)
+
+
 def test_tc_config2_golden(tensor_cores):
     p = W.config2()
     assert PK.digest(api.matmul(8, 8, 8, p.A, p.B)) == G.digests()["config2"]["C"]
