@@ -784,6 +784,8 @@ def serving_benchmark(api, args):
                     tickets[i] = srv.submit_holder(sets[i % npool][(i // npool) % 2])
 
             b0 = srv.stats()["batches"]
+            ph0 = srv.phase_ms()
+            srv.phase_max_ms()  # reset
             th = threading.Thread(target=feeder)
             th.start()
             lat, subs, dones = [], [], []
@@ -807,7 +809,9 @@ def serving_benchmark(api, args):
                                  "submitted_s": (subs[i] - t_first) / 1e9,
                                  "latency_ms": lat[i]} for i in worst],
                     "unit": "requests/s",
-                    "products_per_batch": R / max(1, srv.stats()["batches"] - b0)}
+                    "products_per_batch": R / max(1, srv.stats()["batches"] - b0),
+                    "phase_ms": {k: round(v - ph0[k], 1) for k, v in srv.phase_ms().items()},
+                    "phase_max_ms": {k: round(v, 2) for k, v in srv.phase_max_ms().items()}}
 
         runs = []
         for frac in (0.5, 0.8, 0.95):

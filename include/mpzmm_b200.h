@@ -350,7 +350,9 @@ MPZMM_API int mpzmm_matmul_noalloc(int m, int k, int n,
    batches run join the next batch; a request's residues stay on the device
    for the whole pipeline.  Each slot's pinned staging is allocated once at
    creation and its device memory comes from a stream-ordered pool of the
-   server's own, so no batch synchronises the device.  Each slot has two
+   server's own (a quarter of the budget, at most 32 GB, is taken into it at
+   creation), so no batch synchronises the device or waits for the driver
+   to map memory.  Each slot has two
    streams: batches of small requests run on one of the device's greatest
    stream priority, batches of large ones on one of its least, so a small
    request waits neither inside a large one's batch nor behind its queued
@@ -379,6 +381,9 @@ MPZMM_API int mpzmm_server_stats(mpzmm_server *server, int64_t *batches, int64_t
 /* Scheduler-thread nanoseconds spent in: plan building, input gather and
    copy, kernel launches, result copy-back and scatter (4 values). */
 MPZMM_API int mpzmm_server_phase_ns(mpzmm_server *server, int64_t *ns4);
+/* The longest single batch in each of those phases since the previous call
+   (4 values, nanoseconds); reading resets them. */
+MPZMM_API int mpzmm_server_phase_max_ns(mpzmm_server *server, int64_t *ns4);
 /* Admission window: when a slot frees up while other batches are on the GPU,
    it keeps admitting queued requests for up to this many microseconds
    before launching its batch (default 200; 0 launches at once).  With the

@@ -111,6 +111,7 @@ def lib():
         "mpzmm_server_set_admission_window": (C.c_int, [vp, C.c_int64]),
         "mpzmm_server_destroy": (None, [vp]),
         "mpzmm_server_phase_ns": (C.c_int, [vp, i64p]),
+        "mpzmm_server_phase_max_ns": (C.c_int, [vp, i64p]),
         "mpzmm_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
         "mpzmm_host_free": (C.c_int, [vp]),
         "mpzmm_host_register": (C.c_int, [vp, C.c_size_t]),

@@ -462,6 +462,12 @@ class Server:
         _lib.check(_lib.lib().mpzmm_server_phase_ns(self.handle, C.cast(ns, _lib.i64p)))
         return dict(zip(("build", "upload", "launch", "download"), [x / 1e6 for x in ns]))
 
+    def phase_max_ms(self):
+        """The longest single batch in each phase since the previous call."""
+        ns = (C.c_int64 * 4)()
+        _lib.check(_lib.lib().mpzmm_server_phase_max_ns(self.handle, C.cast(ns, _lib.i64p)))
+        return dict(zip(("build", "upload", "launch", "download"), [x / 1e6 for x in ns]))
+
     def close(self) -> None:
         if self.handle:
             _lib.lib().mpzmm_server_destroy(self.handle)

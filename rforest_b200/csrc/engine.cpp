@@ -493,7 +493,8 @@ int64_t estimate_device_bytes(const ProductSpec& ps, int64_t* host_bytes) {
   return limbs * 8 + res + out + desc;
 }
 
-int Workspace::reserve_staging(size_t stage_limbs, size_t stage_out_words) {
+int Workspace::reserve_staging(size_t stage_limbs, size_t stage_out_words, size_t sizes,
+                               size_t desc_bytes) {
   auto grow = [this](auto** p, size_t& cap, size_t want, size_t elem) -> int {
     if (want <= cap) return kOk;
     if (*p) {
@@ -518,6 +519,8 @@ int Workspace::reserve_staging(size_t stage_limbs, size_t stage_out_words) {
   };
   int st = grow(&h_limbs, hcap_limbs, stage_limbs, 8);
   if (!st) st = grow(&h_out, hcap_out, stage_out_words, 4);
+  if (!st) st = grow(&h_sizes, hcap_sizes, sizes, 4);
+  if (!st) st = grow(&h_desc, hcap_desc, desc_bytes, 1);
   return st;
 }
 

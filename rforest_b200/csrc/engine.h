@@ -115,11 +115,12 @@ struct Workspace {
   // pinned staging of limbs and output words); returns a status.
   int reserve(size_t limbs, size_t res, size_t out_words, size_t sizes, size_t desc_bytes,
               size_t stage_limbs, size_t stage_out_words);
-  // Grows only the pinned staging (limbs, output words) to at least these
-  // counts: a long-lived workspace sized once so that later batches never
-  // allocate pinned memory (cudaMallocHost is slow and cudaFreeHost
-  // synchronises the device).
-  int reserve_staging(size_t stage_limbs, size_t stage_out_words);
+  // Grows only the pinned staging (limbs, output words, result sizes,
+  // descriptor bytes) to at least these counts: a long-lived workspace sized
+  // once so that later batches never allocate pinned memory (cudaMallocHost
+  // is slow and cudaFreeHost synchronises the device).
+  int reserve_staging(size_t stage_limbs, size_t stage_out_words, size_t sizes = 0,
+                      size_t desc_bytes = 0);
   void release_device();  // device buffers only (pinned host buffers stay)
   void release();
   ~Workspace() { release(); }

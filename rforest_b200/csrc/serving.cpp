@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -43,6 +44,12 @@ struct Ticket {
   int status = -1;  // -1 pending
   std::string error;
 };
+
+// pinned result-size and descriptor staging a slot allocates at start: a
+// batch needs 4 bytes an output entry and about 32 bytes an entry and 12 a
+// contraction block, far below these for any batch under the host-data cap
+constexpr size_t kStageSizes = (size_t)1 << 20;
+constexpr size_t kStageDescBytes = (size_t)16 << 20;
 
 struct Slot {
   cudaStream_t stream = nullptr;     // least priority: batches with much data
@@ -89,6 +96,8 @@ struct mpzmm_server {
   // slot-thread time per phase, summed over slots (ns): plan build, input
   // gather + copy, launches, wait + result copy-back + scatter
   int64_t ns_build = 0, ns_upload = 0, ns_launch = 0, ns_download = 0;
+  // the longest single batch in each phase since the last read (ns)
+  int64_t ns_max[4] = {0, 0, 0, 0};
 
   void complete(const std::shared_ptr<Ticket>& t, int status, const std::string& err) {
     t->status = status;
@@ -168,6 +177,9 @@ struct mpzmm_server {
     ns_upload += a2 - a1;
     ns_launch += a3 - a2;
     ns_download += a4 - a3;
+    const int64_t d[4] = {a1 - a0, a2 - a1, a3 - a2, a4 - a3};
+    for (int q = 0; q < 4; ++q)
+      if (d[q] > ns_max[q]) ns_max[q] = d[q];
     return st;
   }
 
@@ -175,7 +187,8 @@ struct mpzmm_server {
     cudaSetDevice(device);
     // pinned staging for a full batch, once (a failure here only means the
     // first batches grow it instead)
-    if (s.ws.reserve_staging((size_t)(batch_host_cap / 8), (size_t)(batch_host_cap / 4)))
+    if (s.ws.reserve_staging((size_t)(batch_host_cap / 8), (size_t)(batch_host_cap / 4),
+                             kStageSizes, kStageDescBytes))
       cudaGetLastError();
     for (;;) {
       std::vector<std::shared_ptr<Ticket>> batch;
@@ -263,6 +276,28 @@ int mpzmm_server_create(mpzmm_server** out, int64_t budget_bytes, int slots, int
       cudaMemPoolDestroy(s->pool);
       return set_error(kErrCuda, std::string("cudaMemPoolSetAttribute: ") +
                                      cudaGetErrorString(e));
+    }
+    // a quarter of the budget, at most 32 GB, taken into the pool at
+    // creation (allocated and freed once): slot workspaces growing later are
+    // served from it without the driver mapping memory, which stalled
+    // saturation runs (730 against 1,680 requests/s on the config-5 pool).
+    // MPZMM_SERVER_PREWARM_GB replaces the amount (0: none).
+    const int64_t prewarm = [budget_bytes] {
+      const char* v = std::getenv("MPZMM_SERVER_PREWARM_GB");
+      if (v) return (int64_t)std::atoi(v) << 30;
+      const int64_t q = budget_bytes / 4;
+      return q < ((int64_t)32 << 30) ? q : ((int64_t)32 << 30);
+    }();
+    if (prewarm > 0 && prewarm < budget_bytes) {
+      cudaStream_t ps = nullptr;
+      void* p = nullptr;
+      if (cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking) == cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&p, (size_t)prewarm, s->pool, ps) == cudaSuccess)
+          cudaFreeAsync(p, ps);
+        cudaStreamSynchronize(ps);
+        cudaStreamDestroy(ps);
+      }
+      cudaGetLastError();
     }
   }
   int least = 0, greatest = 0;
@@ -395,6 +430,16 @@ int mpzmm_server_phase_ns(mpzmm_server* s, int64_t* ns4) {
   ns4[1] = s->ns_upload;
   ns4[2] = s->ns_launch;
   ns4[3] = s->ns_download;
+  return kOk;
+}
+
+int mpzmm_server_phase_max_ns(mpzmm_server* s, int64_t* ns4) {
+  if (!s || !ns4) return set_error(kErrArg, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (int q = 0; q < 4; ++q) {
+    ns4[q] = s->ns_max[q];
+    s->ns_max[q] = 0;
+  }
   return kOk;
 }
 
