@@ -123,3 +123,28 @@ def test_server_admission_window(gpu):
             assert e.value.status == _lib.MPZMM_ERR_ARG
         finally:
             srv.close()
+
+
+def test_server_small_and_large_requests_mixed(gpu):
+    """Small requests (at most 16 MB of host data) and large ones (a 64 x 64
+    by 64 x 64 product of 2^14-bit entries, about 33 MB) queued together:
+    they are batched by class and run on streams of two priorities, and every
+    result still equals the product computed alone.  The phase maxima reset
+    on reading."""
+    small = small_requests(24, seed=23)
+    big = [W.random_product(31, t, 64, 64, 14, 14) for t in range(2)]
+    order = small[:8] + [big[0]] + small[8:16] + [big[1]] + small[16:]
+    alone = [PK.digest(api.matmul(p.m, p.k, p.n, p.A, p.B)) for p in order]
+    srv = api.Server(budget_bytes=0, slots=3, max_batch=8)
+    try:
+        tickets = [srv.submit(p.m, p.k, p.n, p.A, p.B) for p in order]
+        got = [PK.digest(srv.wait(t, 120000)) for t in tickets]
+        assert got == alone
+        mx = srv.phase_max_ms()
+        assert set(mx) == {"build", "upload", "launch", "download"}
+        assert all(v >= 0 for v in mx.values()) and mx["download"] > 0
+        assert all(v == 0 for v in srv.phase_max_ms().values())  # reset by the read
+        for t in tickets:
+            srv.release(t)
+    finally:
+        srv.close()
