@@ -644,7 +644,7 @@ int Plan::prepare(std::vector<ProductSpec> prods) {
     pd.n = (uint16_t)n;
     pd.lgN = (uint16_t)lgN;
     pd.P = (uint16_t)P;
-    pd.pad = (uint16_t)((m >= 3 ? 2 : 0) + (n >= 3 ? 1 : 0));  // contraction tile
+    pd.pad = (uint16_t)contract_tile(m, n);
     n_res_ = (n_res_ + 7) & ~(uint64_t)7;  // 32-byte aligned polynomials (vector loads)
     pd.a_res = n_res_;
     n_res_ += (uint64_t)m * k * poly;

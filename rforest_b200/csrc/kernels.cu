@@ -286,10 +286,15 @@ k_contract(const ProdDesc* __restrict__ prods, const ContractItem* __restrict__ 
   const int N = 1 << d.lgN;
   const uint32_t h = it.h0 + threadIdx.x;
   if (h >= (uint32_t)N) return;
-  switch (d.pad) {  // tile shape, uniform over the CTA
-    case 3: contract_tiles<4, 4>(d, it.prime, h, res); break;
-    case 2: contract_tiles<4, 2>(d, it.prime, h, res); break;
-    case 1: contract_tiles<2, 4>(d, it.prime, h, res); break;
+  switch (d.pad) {  // tile shape 3 (TI - 2) + (TJ - 2), uniform over the CTA
+    case 8: contract_tiles<4, 4>(d, it.prime, h, res); break;
+    case 7: contract_tiles<4, 3>(d, it.prime, h, res); break;
+    case 6: contract_tiles<4, 2>(d, it.prime, h, res); break;
+    case 5: contract_tiles<3, 4>(d, it.prime, h, res); break;
+    case 4: contract_tiles<3, 3>(d, it.prime, h, res); break;
+    case 3: contract_tiles<3, 2>(d, it.prime, h, res); break;
+    case 2: contract_tiles<2, 4>(d, it.prime, h, res); break;
+    case 1: contract_tiles<2, 3>(d, it.prime, h, res); break;
     default: contract_tiles<2, 2>(d, it.prime, h, res); break;
   }
 }

@@ -112,7 +112,7 @@ struct ProdDesc {
   uint16_t m, k, n;
   uint16_t lgN;
   uint16_t P;
-  uint16_t pad;        // contraction register tile: bit 1 -> 4 rows, bit 0 -> 4 cols
+  uint16_t pad;        // contraction register tile TI x TJ (2..4 each): 3 (TI - 2) + TJ - 2
 };
 
 // Work item of the contraction: one product, one prime, one frequency block.

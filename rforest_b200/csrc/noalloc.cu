@@ -183,7 +183,7 @@ extern "C" int mpzmm_matmul_noalloc(int m, int k, int n, const uint64_t* d_a_lim
   pd->n = (uint16_t)n;
   pd->lgN = (uint16_t)lgN;
   pd->P = (uint16_t)P;
-  pd->pad = (uint16_t)((m >= 3 ? 2 : 0) + (n >= 3 ? 1 : 0));  // contraction tile
+  pd->pad = (uint16_t)contract_tile(m, n);  // contraction tile
   pd->a_res = 0;
   pd->b_res = (uint64_t)na * poly;
   pd->c_res = (uint64_t)(na + nb) * poly;

@@ -44,6 +44,9 @@ int ceil_log2(uint64_t x);
 // the symmetric CRT residue is c itself, with the margin the rounded
 // explicit CRT needs.  Returns false if no supported (P, r, lgN) exists.
 bool choose_params(int64_t a_bits, int64_t b_bits, int m, int k, int n, Params* out);
+// Register tile of the CUDA-core contraction for an m x n product, encoded
+// as 3 (TI - 2) + (TJ - 2) with 2 <= TI, TJ <= 4 (ProdDesc::pad).
+int contract_tile(int m, int n);
 
 // ceil((a_bits + b_bits + ceil(log2 k) + 1) / 64)
 int64_t output_limbs(int k, int64_t a_bits, int64_t b_bits);
