@@ -464,6 +464,7 @@ def main():
         api.set_contract_mode(modes[args.contract])
         comparisons["mod_reduction"] = mod_benchmark(api)
         comparisons["config4"] = config4_benchmark(api, torch, stream)
+        comparisons["fixed_b"] = fixed_b_benchmark(api, triples[:512])
 
     if rank == 0:
         # roofline of the dominant stage (3-pass model, reference parameters)
@@ -642,6 +643,35 @@ def config4_benchmark(api, torch, stream, reps=3):
             plan.close()
     finally:
         api.set_contract_mode(saved)
+    return out
+
+
+def fixed_b_benchmark(api, triples, reps=5):
+    """A plan that keeps B's transforms: one execute after new A values
+    (upload_a, B's split and transforms skipped) against one after a full
+    upload, per stage, device time (CUDA events on the execute stream), and
+    the results checked against the ordinary entry point."""
+    from rforest_b200 import packed as PK
+    plan = api.Plan(triples, fixed_b=True)
+    plan.set_timing(True)
+    plan.execute()
+    plan.stage_times()  # drop the first execute
+    out = {}
+    names = ("split_fwd_ntt", "contract", "inv_ntt", "crt_recompose")
+    for name, up in (("full_upload", plan.upload), ("upload_a", plan.upload_a)):
+        for _ in range(reps):
+            up()
+            plan.execute()
+        ms, _, ex = plan.stage_times()
+        ex = max(1, ex)
+        out[name] = {"stages_ms": {k: round(v / ex, 3) for k, v in zip(names, ms)},
+                     "ms": round(sum(ms) / ex, 3)}
+    got = [PK.digest(c) for c in plan.download()]
+    want = [PK.digest(api.matmul(m, k, n, A, B)) for (m, k, n, A, B) in triples]
+    plan.close()
+    out["products"] = len(triples)
+    out["verified"] = got == want
+    out["timing"] = "device, CUDA events per stage, mean of %d executes" % reps
     return out
 
 

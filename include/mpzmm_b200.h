@@ -284,6 +284,18 @@ MPZMM_API int mpzmm_plan_download(mpzmm_plan *plan, void *stream);
    and copies them to the device.  Asynchronous on `stream`. */
 MPZMM_API int mpzmm_plan_upload(mpzmm_plan *plan, void *stream);
 MPZMM_API void mpzmm_plan_destroy(mpzmm_plan *plan);
+/* A plan that keeps B's transforms across executes (the same B times many
+   A): the first execute after create or mpzmm_plan_upload splits and
+   transforms both operands, later executes transform only A.
+   mpzmm_plan_upload_a re-reads only the A operands (same shapes and signed
+   limb counts),
+   so their products with the same B skip B's split and transforms;
+   mpzmm_plan_upload re-reads both.  Such a plan does not use graph mode.
+   (The reference re-splits and re-transforms B on every call,
+   src/lib/hwmpz.c:80-105.) */
+MPZMM_API int mpzmm_plan_create_fixed_b(mpzmm_plan **plan, int count,
+                                        const mpzmm_product *products, void *stream);
+MPZMM_API int mpzmm_plan_upload_a(mpzmm_plan *plan, void *stream);
 
 /* CUDA-graph mode (off by default): the first execute captures every launch
    of the plan into a CUDA graph on its stream; later executes replay it as one

@@ -93,6 +93,8 @@ def lib():
         "mpzmm_plan_execute": (C.c_int, [vp, vp]),
         "mpzmm_plan_download": (C.c_int, [vp, vp]),
         "mpzmm_plan_upload": (C.c_int, [vp, vp]),
+        "mpzmm_plan_create_fixed_b": (C.c_int, [C.POINTER(vp), C.c_int, C.POINTER(Product), vp]),
+        "mpzmm_plan_upload_a": (C.c_int, [vp, vp]),
         "mpzmm_plan_destroy": (None, [vp]),
         "mpzmm_plan_set_timing": (C.c_int, [vp, C.c_int]),
         "mpzmm_plan_set_graph": (C.c_int, [vp, C.c_int]),

@@ -353,12 +353,28 @@ class Mod:
 class Plan:
     """A device-resident batch: inputs uploaded once, executed many times."""
 
-    def __init__(self, products: Sequence[ProductIn], stream=None):
+    def __init__(self, products: Sequence[ProductIn], stream=None, fixed_b: bool = False):
+        """fixed_b: keep B's transforms across executes (mpzmm_plan_create_fixed_b);
+        set new A values with set_a() and upload_a()."""
         self.holders = [_Holder(*p) for p in products]
         self.arr = (_lib.Product * len(self.holders))(*[h.struct for h in self.holders])
         self.handle = C.c_void_p()
-        _lib.check(_lib.lib().mpzmm_plan_create(C.byref(self.handle), len(self.holders),
-                                                self.arr, _stream_arg(stream)))
+        create = (_lib.lib().mpzmm_plan_create_fixed_b if fixed_b
+                  else _lib.lib().mpzmm_plan_create)
+        _lib.check(create(C.byref(self.handle), len(self.holders), self.arr,
+                          _stream_arg(stream)))
+
+    def set_a(self, index: int, A: Packed) -> None:
+        """New A values for product `index` with the same signed limb counts
+        (the plan's descriptors hold sizes and signs), read by the next
+        upload() or upload_a()."""
+        h = self.holders[index]
+        if not np.array_equal(np.asarray(A.sizes, dtype=np.int32), h.asz):
+            raise ValueError("new A must have the same signed limb counts")
+        np.copyto(h.al[:A.limbs.size], A.limbs)
+
+    def upload_a(self, stream=None) -> None:
+        _lib.check(_lib.lib().mpzmm_plan_upload_a(self.handle, _stream_arg(stream)))
 
     def execute(self, stream=None) -> None:
         _lib.check(_lib.lib().mpzmm_plan_execute(self.handle, _stream_arg(stream)))

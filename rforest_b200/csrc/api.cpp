@@ -457,8 +457,8 @@ int mpzmm_chain(int count, const mpzmm_matrix* mats, uint64_t* c_limbs, const in
   return run_chain(std::move(steps), pick_stream(stream));
 }
 
-int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* products,
-                      void* stream) {
+static int plan_create(mpzmm_plan** plan, int count, const mpzmm_product* products,
+                       bool fixed_b, void* stream) {
   if (!plan) return set_error(kErrArg, "null plan pointer");
   *plan = nullptr;
   if (count < 0 || (count > 0 && !products)) return set_error(kErrArg, "bad product list");
@@ -467,10 +467,26 @@ int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* product
   std::vector<ProductSpec> specs;
   if ((st = build_specs_packed(count, products, &specs))) return st;
   std::unique_ptr<mpzmm_plan> p(new mpzmm_plan);
+  p->plan.set_fixed_b(fixed_b);
   if ((st = p->plan.build(std::move(specs)))) return st;
   if ((st = p->plan.upload(pick_stream(stream)))) return st;
   *plan = p.release();
   return kOk;
+}
+
+int mpzmm_plan_create(mpzmm_plan** plan, int count, const mpzmm_product* products,
+                      void* stream) {
+  return plan_create(plan, count, products, false, stream);
+}
+
+int mpzmm_plan_create_fixed_b(mpzmm_plan** plan, int count, const mpzmm_product* products,
+                              void* stream) {
+  return plan_create(plan, count, products, true, stream);
+}
+
+int mpzmm_plan_upload_a(mpzmm_plan* plan, void* stream) {
+  if (!plan) return set_error(kErrArg, "null plan");
+  return plan->plan.upload_a(pick_stream(stream));
 }
 
 int mpzmm_plan_execute(mpzmm_plan* plan, void* stream) {

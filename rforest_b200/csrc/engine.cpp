@@ -661,14 +661,21 @@ int Plan::prepare(std::vector<ProductSpec> prods) {
     const bool use_tc = contract_tc_eligible(m, k, n) && lgN >= 3 && lgN <= kMaxLgNOneCta &&
                         (mode == 2 || (mode == 0 && context().tc_pref[tc_bucket_k(k)]
                                                                      [tc_bucket_mn(m, n)] == 1));
-    // one class per product; operands of tensor-core products (blocked
-    // layout) get launches of their own, so the plain kernels stay as lean
-    Group& fg = fwdg[{lgN, P * 16 + (r + 29) / 30 + (use_tc ? 1024 : 0)}];
-    fg.tiled = use_tc;
-    fg.P = P;
-    fg.lgN = lgN;
-    if (r > fg.max_r) fg.max_r = r;
+    if (fixed_b_ && ps.dev_a)
+      return set_error(kErrArg, "a plan that keeps B's transforms takes host operands only");
     for (int side = 0; side < 2; ++side) {
+      // one class per product; operands of tensor-core products (blocked
+      // layout) get launches of their own, so the plain kernels stay as
+      // lean, and so do B operands whose transforms the plan keeps
+      const bool b_only = fixed_b_ && side == 1;
+      Group& fg =
+          fwdg[{lgN, P * 16 + (r + 29) / 30 + (use_tc ? 1024 : 0) + (b_only ? 2048 : 0)}];
+      fg.tiled = use_tc;
+      fg.b_only = b_only;
+      fg.P = P;
+      fg.lgN = lgN;
+      if (r > fg.max_r) fg.max_r = r;
+      if (fixed_b_) host_end = nullptr;  // runs never mix the two operands
       const auto& ents = side ? ps.b : ps.a;
       const uint64_t base = side ? pd.b_res : pd.a_res;
       if (!side && ps.dev_a) {
@@ -727,7 +734,8 @@ int Plan::prepare(std::vector<ProductSpec> prods) {
             run_pinned_end = range_end(pinned, d, (size_t)nl * 8);
             const uint64_t want = (reinterpret_cast<uintptr_t>(d) >> 3) & 31;
             n_limbs_ += (want - n_limbs_) & 31;
-            in_runs_.push_back(Run{d, n_limbs_, (uint64_t)nl, 0, run_pinned_end != 0, 1, 0});
+            in_runs_.push_back(
+                Run{d, n_limbs_, (uint64_t)nl, 0, run_pinned_end != 0, 1, 0, side == 1});
           }
           host_end = d + nl;
         }
@@ -836,10 +844,11 @@ int Plan::prepare(std::vector<ProductSpec> prods) {
       const bool team = ((int64_t)1 << g.lgN) <= (int64_t)fwd_team_points();
       // a CTA's shared memory follows the launch's largest class, so classes
       // above the team size get launches of their own
-      Group& v = var[{(team ? 0 : g.lgN) + (g.tiled ? 64 : 0), D}];
+      Group& v = var[{(team ? 0 : g.lgN) + (g.tiled ? 64 : 0) + (g.b_only ? 128 : 0), D}];
       v.batched = true;
       v.team = team;
       v.tiled = g.tiled;
+      v.b_only = g.b_only;
       v.D = D;
       if (g.lgN > v.max_lgN) v.max_lgN = g.lgN;
       const size_t G = team ? (size_t)(fwd_team_points() >> g.lgN) : 1;
@@ -1027,7 +1036,13 @@ void Plan::plan_transfers() {
 }
 
 int Plan::upload(cudaStream_t st) {
+  b_valid_ = false;  // B's limbs are read again: its transforms follow at the next execute
+  return upload_sides(st, false);
+}
+
+int Plan::upload_sides(cudaStream_t st, bool a_only) {
   if (!built_) return set_error(kErrState, "plan not built");
+  if (a_only && !fixed_b_) return set_error(kErrState, "the plan does not keep B's transforms");
   if (desc_bytes_)
     CU(cudaMemcpyAsync(ws_->d_desc, ws_->h_desc, desc_bytes_, cudaMemcpyHostToDevice, st),
        "H2D descriptors");
@@ -1040,9 +1055,11 @@ int Plan::upload(cudaStream_t st) {
          "D2D limbs");
   for (const DevFix& f : dev_fixes_)
     CU(launch_fix_sizes(d_fwd_ + f.first_fwd, (int)f.count, f.sizes, st), "size fix-up launch");
+  // a_only: B's runs stay as they are (its transforms are kept)
+  auto skip = [a_only](const Run& r) { return a_only && r.b; };
   // straight copies first, so the DMA runs while the staged runs are gathered
   for (const Run& r : in_runs_)
-    if (r.direct)
+    if (r.direct && !skip(r))
       CU(cudaMemcpyAsync(ws_->d_limbs + r.dev, r.host, r.n * 8, cudaMemcpyHostToDevice, st),
          "H2D limbs");
   if (!stage_limbs_) return kOk;
@@ -1054,7 +1071,7 @@ int Plan::upload(cudaStream_t st) {
   constexpr uint64_t kPiece = (4ull << 20) / 8;
   std::vector<Piece> pieces;
   for (const Run& r : in_runs_) {
-    if (r.direct) continue;
+    if (r.direct || skip(r)) continue;
     for (uint64_t o = 0; o < r.n; o += kPiece)
       pieces.push_back(Piece{static_cast<const uint64_t*>(r.host) + o, r.stage + o,
                              r.n - o < kPiece ? r.n - o : kPiece});
@@ -1069,13 +1086,14 @@ int Plan::upload(cudaStream_t st) {
   // the gap words are padding nobody reads
   size_t i = 0;
   while (i < in_runs_.size()) {
-    if (in_runs_[i].direct) {
+    if (in_runs_[i].direct || skip(in_runs_[i])) {
       ++i;
       continue;
     }
     uint64_t dev = in_runs_[i].dev, stg = in_runs_[i].stage, n = in_runs_[i].n;
     size_t j = i + 1;
-    while (j < in_runs_.size() && !in_runs_[j].direct && in_runs_[j].dev >= dev + n &&
+    while (j < in_runs_.size() && !in_runs_[j].direct && !skip(in_runs_[j]) &&
+           in_runs_[j].dev >= dev + n &&
            in_runs_[j].dev - (dev + n) == in_runs_[j].stage - (stg + n)) {
       n = in_runs_[j].dev + in_runs_[j].n - dev;
       ++j;
@@ -1089,7 +1107,7 @@ int Plan::upload(cudaStream_t st) {
 
 int Plan::execute(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
-  if (!use_graph_ || timing_) return launch_all(st, timing_);
+  if (!use_graph_ || timing_ || fixed_b_) return launch_all(st, timing_);
   if (!graph_exec_) {
     if (ws_->fanout) {  // no stream or event creation inside the capture
       const int e0 = ws_->ensure_side();
@@ -1152,8 +1170,12 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
     }
     CU(cudaEventRecord(ev[0], st), "cudaEventRecord");
   }
-  int r = fan_out(ws_, st, (int)fwd_groups_.size(), [&](int i, cudaStream_t s) -> int {
-    const Group& g = fwd_groups_[i];
+  // a plan that keeps B's transforms skips B's launches while they are current
+  std::vector<const Group*> fwd_run;
+  for (const Group& g : fwd_groups_)
+    if (!(g.b_only && b_valid_)) fwd_run.push_back(&g);
+  int r = fan_out(ws_, st, (int)fwd_run.size(), [&](int i, cudaStream_t s) -> int {
+    const Group& g = *fwd_run[i];
     if (g.large)
       CU(launch_large_fwd(d_fwd_, d_idx_ + g.idx_off, (int)g.idx.size(), g.lgN, g.D,
                           ws_->d_limbs, ws_->d_res, ctx.d_twf, ctx.twist_f, s),
@@ -1205,6 +1227,7 @@ int Plan::launch_all(cudaStream_t st, bool timed) {
   });
   if (r != kOk) return r;
   if (timed) CU(cudaEventRecord(ev[4], st), "cudaEventRecord");
+  b_valid_ = fixed_b_;
   return kOk;
 }
 

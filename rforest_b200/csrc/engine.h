@@ -259,6 +259,13 @@ class Plan {
   // from the caller's memory where it is pinned memory known to the library,
   // through the pinned staging buffer otherwise.
   int upload(cudaStream_t st);
+  // Keep B's transforms (call before build): B operands get forward launches
+  // of their own, which run at the first execute after an upload() and are
+  // skipped by later executes; upload_a() re-reads only the A operands, so
+  // their products with the same B need only A's split and transforms.
+  // Such a plan takes host operands only and does not capture CUDA graphs.
+  void set_fixed_b(bool on) { fixed_b_ = on; }
+  int upload_a(cudaStream_t st) { return upload_sides(st, true); }
   // Runs split+fwd NTT, contraction, inverse NTT, CRT+recompose.  With
   // graph mode on (and timing off) the launches are captured into a CUDA
   // graph on the first call and replayed as one graph launch afterwards.
@@ -304,6 +311,7 @@ class Plan {
     bool team = false;
     bool large = false;    // four-step transform (2^lgN above one CTA)
     bool tiled = false;    // forward: operands of tensor-core products (blocked layout)
+    bool b_only = false;   // forward: B operands of a plan that keeps their transforms
     int D = 0;
     int max_lgN = 0;
     std::vector<CtaItem> items;
@@ -337,6 +345,7 @@ class Plan {
     uint64_t dev, n, stage;
     bool direct;
     uint64_t rows, pitch;
+    bool b = false;  // input run of B operands (plans that keep B's transforms)
   };
   std::vector<Run> in_runs_, out_runs_;
   // device-resident operands: limb spans copied on the device, and the
@@ -380,6 +389,9 @@ class Plan {
   bool timing_ = false;
   std::vector<cudaEvent_t> events_;  // kStages + 1 per timed execute
   bool use_graph_ = false;
+  bool fixed_b_ = false;
+  bool b_valid_ = false;  // B's transforms in device memory match its limbs
+  int upload_sides(cudaStream_t st, bool a_only);
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   int launch_all(cudaStream_t st, bool timed);

@@ -108,6 +108,48 @@ def test_plan_graph_replay_with_new_inputs(gpu):
     plan.close()
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_plan_keeps_b_transforms(gpu, mode):
+    """A plan that keeps B's transforms (the same B times many A), on CUDA
+    cores and on tensor cores: after upload_a the products of new A values
+    with the kept B are exact, a B changed in host memory is not read by
+    upload_a, and a full upload brings it in."""
+    api.set_contract_mode(mode)
+    try:
+        prods = [W.random_product(37, t, 2, 12, 8, 14) for t in range(10)]
+        plan = api.Plan([(p.m, p.k, p.n, p.A, p.B) for p in prods], fixed_b=True)
+
+        def want(bls):
+            out = []
+            for h, p, bl in zip(plan.holders, prods, bls):
+                A = PK.Packed(h.al, h.ao, h.asz)
+                B = PK.Packed(bl, h.bo, h.bsz)
+                out.append(PK.digest(api.matmul(p.m, p.k, p.n, A, B)))
+            return out
+
+        kept = [h.bl.copy() for h in plan.holders]
+        plan.execute()
+        assert [PK.digest(c) for c in plan.download()] == want(kept)
+        for rnd in range(2):  # new A values (same sizes and signs), B's transforms kept
+            for h in plan.holders:
+                h.al ^= np.uint64(1 << rnd)
+            plan.upload_a()
+            plan.execute()
+            assert [PK.digest(c) for c in plan.download()] == want(kept)
+        for h in plan.holders:  # B changes in host memory: upload_a leaves it
+            h.bl ^= np.uint64(1)
+        plan.upload_a()
+        plan.execute()
+        assert [PK.digest(c) for c in plan.download()] == want(kept)
+        plan.upload()  # a full upload reads the new B, transformed at the next execute
+        plan.execute()
+        plan.execute()
+        assert [PK.digest(c) for c in plan.download()] == want([h.bl for h in plan.holders])
+        plan.close()
+    finally:
+        api.set_contract_mode(0)
+
+
 def test_server_admission_window(gpu):
     """The admission window changes how requests are batched, never the
     results; a negative window is refused."""
