@@ -48,6 +48,8 @@ extern "C" {
 #define MPZMM_ERR_STATE 6      /* not set up, or object in the wrong state */
 #define MPZMM_ERR_TIMEOUT 7    /* a bounded wait gave up                  */
 #define MPZMM_ERR_BUSY 8       /* admission refused (queue/memory full)   */
+#define MPZMM_ERR_BOUNDS 9     /* debug bounds check: a descriptor outside
+                                  the workspace (nothing was launched)     */
 
 /* ======================================================================
  * 1. Reference-compatible API (src/include/hwmpz.h)
@@ -110,9 +112,16 @@ MPZMM_API int mpzmm_setup(int device);
    MPZMM_OPT_CHUNK_LIMBS sets the input limbs per chunk of a pipelined
    one-shot batch (mpzmm_matmul_batch): 0 (default) chooses a 32nd of the
    batch, kept between 2^22 and 2^26 limbs; a batch no larger than one
-   chunk runs unchunked. */
+   chunk runs unchunked.
+   MPZMM_OPT_CHECK_BOUNDS (debug, default 0; environment variable
+   MPZMM_CHECK_BOUNDS=1): before every execute of a plan (batches, chains,
+   server batches included) a kernel checks every descriptor's extents
+   against the workspace and writes a status word; on a violation the call
+   returns MPZMM_ERR_BOUNDS without launching anything else.  It costs a
+   stream synchronisation per execute. */
 #define MPZMM_OPT_CONTRACT 1
 #define MPZMM_OPT_CHUNK_LIMBS 2
+#define MPZMM_OPT_CHECK_BOUNDS 3
 /* Failure injection, for tests of a caller's error handling (no counterpart
    in the reference; nothing here faults a GPU).  MPZMM_OPT_TEST_STALL_TC:
    the next `value` tensor-core contraction launches issue no tensor work,

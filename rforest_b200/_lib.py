@@ -18,9 +18,11 @@ MPZMM_ERR_NOMEM = 5
 MPZMM_ERR_STATE = 6
 MPZMM_ERR_TIMEOUT = 7
 MPZMM_ERR_BUSY = 8
+MPZMM_ERR_BOUNDS = 9
 
 MPZMM_OPT_CONTRACT = 1
 MPZMM_OPT_CHUNK_LIMBS = 2
+MPZMM_OPT_CHECK_BOUNDS = 3
 MPZMM_OPT_TEST_STALL_TC = 100
 MPZMM_OPT_TEST_FAIL_ALLOC = 101
 CONTRACT_AUTO, CONTRACT_CUDA_CORES, CONTRACT_TENSOR_CORES = 0, 1, 2

@@ -123,6 +123,11 @@ int mpzmm_set_option(int option, int value) {
     context().chunk_limbs = value;
     return kOk;
   }
+  if (option == MPZMM_OPT_CHECK_BOUNDS) {
+    if (value < 0 || value > 1) return set_error(kErrArg, "bounds check must be 0 or 1");
+    context().check_bounds = value != 0;
+    return kOk;
+  }
   if (option == MPZMM_OPT_TEST_STALL_TC) {
     if (value < 0) return set_error(kErrArg, "count must be >= 0");
     set_test_stall_tc(value);
@@ -226,6 +231,7 @@ int mpzmm_autotune(void* stream, float* ms_out) {
 int mpzmm_get_option(int option) {
   if (option == MPZMM_OPT_CONTRACT) return context().contract_mode;
   if (option == MPZMM_OPT_CHUNK_LIMBS) return (int)context().chunk_limbs;
+  if (option == MPZMM_OPT_CHECK_BOUNDS) return context().check_bounds ? 1 : 0;
   if (option == MPZMM_OPT_TEST_STALL_TC) return test_stall_tc();
   if (option == MPZMM_OPT_TEST_FAIL_ALLOC) return test_fail_alloc();
   return -1;

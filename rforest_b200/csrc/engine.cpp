@@ -243,6 +243,7 @@ int ensure_setup(int device) {
   }
   CU(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking), "cudaStreamCreate");
   g_ctx.ws = new Workspace;
+  if (const char* cb = std::getenv("MPZMM_CHECK_BOUNDS")) g_ctx.check_bounds = cb[0] == '1';
   if (const char* cm = std::getenv("MPZMM_CONTRACT")) {
     const int v = std::atoi(cm);
     if (v >= 0 && v <= 2) g_ctx.contract_mode = v;
@@ -584,6 +585,7 @@ int Plan::build(std::vector<ProductSpec> prods, Workspace* ws) {
 
 int Plan::prepare(std::vector<ProductSpec> prods) {
   if (built_ || prepared_) return set_error(kErrState, "plan already built");
+  check_bounds_ = context().check_bounds;
   prods_ = std::move(prods);
   const int block_freqs = contract_block_freqs();
   params_.resize(prods_.size());
@@ -1105,8 +1107,35 @@ int Plan::upload_sides(cudaStream_t st, bool a_only) {
   return kOk;
 }
 
+// The debug bounds check: every descriptor's extents against the
+// workspace, on the device, before any other kernel of the execute runs; a
+// violation is reported as MPZMM_ERR_BOUNDS and nothing else is launched.
+int Plan::check_bounds(cudaStream_t st) {
+  BoundsCaps caps;
+  caps.limbs = ws_->cap_limbs;
+  caps.res = ws_->cap_res;
+  caps.out_words = ws_->cap_out;
+  caps.sizes = ws_->cap_sizes;
+  CU(launch_check_bounds(d_fwd_, (int)fwd_.size(), d_inv_, (int)inv_.size(), d_pd_,
+                         (int)pd_.size(), caps, ws_->d_status, st),
+     "bounds check launch");
+  CU(cudaMemcpyAsync(ws_->h_status, ws_->d_status, sizeof(int), cudaMemcpyDeviceToHost, st),
+     "D2H status");
+  CU(cudaStreamSynchronize(st), "bounds check");
+  if (*ws_->h_status == 2) {
+    *ws_->h_status = 0;
+    CU(cudaMemsetAsync(ws_->d_status, 0, sizeof(int), st), "clear status");
+    return set_error(kErrBounds, "debug bounds check: a descriptor lies outside the workspace");
+  }
+  return kOk;
+}
+
 int Plan::execute(cudaStream_t st) {
   if (!built_) return set_error(kErrState, "plan not built");
+  if (check_bounds_) {
+    const int r = check_bounds(st);
+    if (r) return r;
+  }
   if (!use_graph_ || timing_ || fixed_b_) return launch_all(st, timing_);
   if (!graph_exec_) {
     if (ws_->fanout) {  // no stream or event creation inside the capture

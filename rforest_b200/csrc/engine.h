@@ -29,6 +29,7 @@ enum Status : int {
   kErrState = 6,
   kErrTimeout = 7,
   kErrBusy = 8,
+  kErrBounds = 9,
 };
 
 int set_error(int status, const std::string& msg);
@@ -147,6 +148,7 @@ struct Context {
   // contraction engine: 0 automatic (tensor cores from kTcMinK terms on),
   // 1 CUDA cores only, 2 tensor cores wherever the shape allows
   int contract_mode = 0;
+  bool check_bounds = false;  // MPZMM_OPT_CHECK_BOUNDS (env MPZMM_CHECK_BOUNDS)
   // measured engine choice per size class (term-count bucket k <= 8, 16, 32,
   // 64 by row/column bucket max(m, n) <= 4, 8, 16, 32, 64) in automatic
   // mode: -1 not measured (CUDA cores), 0 CUDA cores, 1 tensor cores;
@@ -390,6 +392,8 @@ class Plan {
   std::vector<cudaEvent_t> events_;  // kStages + 1 per timed execute
   bool use_graph_ = false;
   bool fixed_b_ = false;
+  bool check_bounds_ = false;  // the debug bounds check runs before every execute
+  int check_bounds(cudaStream_t st);
   bool b_valid_ = false;  // B's transforms in device memory match its limbs
   int upload_sides(cudaStream_t st, bool a_only);
   cudaGraph_t graph_ = nullptr;

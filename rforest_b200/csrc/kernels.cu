@@ -2007,6 +2007,53 @@ cudaError_t launch_contract(const ProdDesc* prods, const ContractItem* items, in
 
 int contract_block_freqs() { return kContractThreads; }
 
+__device__ __forceinline__ bool fwd_in_bounds(const FwdDesc& f, const BoundsCaps& c) {
+  if (f.lgN > kMaxLgN || f.P > kMaxPrimes) return false;
+  const uint64_t nl = f.size < 0 ? (uint64_t)(-(int64_t)f.size) : (uint64_t)f.size;
+  if (f.limb_off + nl > c.limbs) return false;
+  if (f.tile_np && f.tile_e >= f.tile_np) return false;
+  // the plain layout: P polynomials of N words; blocked: the operand's block
+  const uint64_t words = ((uint64_t)f.P << f.lgN) * (f.tile_np ? f.tile_np : 1u);
+  return f.res_off + words <= c.res;
+}
+
+__device__ __forceinline__ bool inv_in_bounds(const InvDesc& v, const BoundsCaps& c) {
+  if (v.lgN > kMaxLgN || v.P > kMaxPrimes) return false;
+  return v.res_off + ((uint64_t)v.P << v.lgN) <= c.res &&
+         v.out_word + v.out_words <= c.out_words && v.entry < c.sizes;
+}
+
+__device__ __forceinline__ bool prod_in_bounds(const ProdDesc& d, const BoundsCaps& c) {
+  if (d.lgN > kMaxLgN || d.P > kMaxPrimes) return false;
+  const uint64_t poly = (uint64_t)d.P << d.lgN;
+  return d.a_res + (uint64_t)d.m * d.k * poly <= c.res &&
+         d.b_res + (uint64_t)d.k * d.n * poly <= c.res &&
+         d.c_res + (uint64_t)d.m * d.n * poly <= c.res;
+}
+
+__global__ void k_check_bounds(const FwdDesc* __restrict__ fwd, int nfwd,
+                               const InvDesc* __restrict__ inv, int ninv,
+                               const ProdDesc* __restrict__ prods, int nprods, BoundsCaps caps,
+                               int* __restrict__ status) {
+  const int total = nfwd + ninv + nprods;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const bool ok = i < nfwd          ? fwd_in_bounds(fwd[i], caps)
+                    : i < nfwd + ninv ? inv_in_bounds(inv[i - nfwd], caps)
+                                      : prod_in_bounds(prods[i - nfwd - ninv], caps);
+    if (!ok) atomicExch(status, 2);
+  }
+}
+
+cudaError_t launch_check_bounds(const FwdDesc* fwd, int nfwd, const InvDesc* inv, int ninv,
+                                const ProdDesc* prods, int nprods, BoundsCaps caps, int* status,
+                                cudaStream_t st) {
+  const int total = nfwd + ninv + nprods;
+  if (total <= 0) return cudaSuccess;
+  const int blocks = (total + 255) / 256 < 1184 ? (total + 255) / 256 : 1184;
+  k_check_bounds<<<blocks, 256, 0, st>>>(fwd, nfwd, inv, ninv, prods, nprods, caps, status);
+  return cudaGetLastError();
+}
+
 bool contract_tc_eligible(int m, int k, int n) {
   return m >= 1 && m <= tc::kMaxM && k >= 1 && k <= tc::kMaxK && n >= 1 && n <= tc::kMaxN;
 }

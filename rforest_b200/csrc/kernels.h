@@ -69,6 +69,16 @@ cudaError_t launch_mod_finish(int count, int n, const uint64_t* xl, const int64_
 // consecutive frequencies.  *status is set to 1 if a bounded wait gave up.
 // stall != 0 (failure-path tests only) issues no tensor work, so every CTA's
 // wait runs out.
+// Debug check (MPZMM_OPT_CHECK_BOUNDS): every forward, inverse and product
+// descriptor's extents against the workspace capacities (limbs, residue
+// words, output words, result sizes); a thread that finds one outside sets
+// *status to 2 and touches nothing else.
+struct BoundsCaps {
+  uint64_t limbs, res, out_words, sizes;
+};
+cudaError_t launch_check_bounds(const FwdDesc* fwd, int nfwd, const InvDesc* inv, int ninv,
+                                const ProdDesc* prods, int nprods, BoundsCaps caps, int* status,
+                                cudaStream_t st);
 bool contract_tc_eligible(int m, int k, int n);
 int contract_tc_freqs();
 int tc_smem_bytes(int m, int k, int n, int F);

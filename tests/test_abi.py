@@ -131,6 +131,16 @@ def test_failure_injection_options_host_only(product_lib):
         assert L.mpzmm_get_option(opt) == 0
 
 
+def test_bounds_check_option_host_only(product_lib):
+    """The debug bounds-check option is host state: 0 or 1, read back."""
+    L = product_lib
+    assert L.mpzmm_set_option(_lib.MPZMM_OPT_CHECK_BOUNDS, 2) == _lib.MPZMM_ERR_ARG
+    assert L.mpzmm_set_option(_lib.MPZMM_OPT_CHECK_BOUNDS, 1) == _lib.MPZMM_OK
+    assert L.mpzmm_get_option(_lib.MPZMM_OPT_CHECK_BOUNDS) == 1
+    assert L.mpzmm_set_option(_lib.MPZMM_OPT_CHECK_BOUNDS, 0) == _lib.MPZMM_OK
+    assert L.mpzmm_get_option(_lib.MPZMM_OPT_CHECK_BOUNDS) == 0
+
+
 def test_reference_drivers_link_against_the_library():
     """Where the reference tree exists, its own tests/test_matmul.c and
     benchmark/bench_matmul.c compile unmodified with this library's header

@@ -10,6 +10,10 @@
 * A host allocation failure: MPZMM_OPT_TEST_FAIL_ALLOC makes the next
   workspace allocation report out-of-memory (MPZMM_ERR_NOMEM) before any
   CUDA allocation is attempted; the next call succeeds.
+* The debug bounds check (MPZMM_OPT_CHECK_BOUNDS): a kernel checks every
+  descriptor against the workspace before each execute and writes a status
+  word (MPZMM_ERR_BOUNDS, nothing else launched).  No test plants a bad
+  descriptor on the GPU; the check is shown to pass every entry point.
 
 The reference has no error reporting to compare with: it asserts or exits
 (alexp616/rforest src/lib/hwmpz.c:69,146).
@@ -18,7 +22,7 @@ import random
 
 import pytest
 
-from rforest_b200 import _lib, api, packed as PK
+from rforest_b200 import _lib, api, packed as PK, workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -85,3 +89,44 @@ def test_allocation_failure_reports_and_recovers(gpu):
     finally:
         _opt(_lib.MPZMM_OPT_TEST_FAIL_ALLOC, 0)
     assert api.matmul(3, 3, 3, A, B).to_ints() == want
+
+
+def test_debug_bounds_check_passes_every_entry_point(gpu):
+    """With the debug bounds check on, every plan execute first checks all
+    descriptors against its workspace on the device (a status word, nothing
+    else touched); on correct plans it finds nothing, and the results of a
+    product, a pipelined batch, a chain and server batches stay exact."""
+    L = _lib.lib()
+    assert L.mpzmm_set_option(_lib.MPZMM_OPT_CHECK_BOUNDS, 1) == _lib.MPZMM_OK
+    try:
+        rng = random.Random(99)
+        Ai = [rng.randrange(-(1 << 900), 1 << 900) for _ in range(6)]
+        Bi = [rng.randrange(-(1 << 700), 1 << 700) for _ in range(12)]
+        C = api.matmul(2, 3, 4, PK.from_ints(Ai), PK.from_ints(Bi))
+        assert C.to_ints() == [sum(Ai[i * 3 + l] * Bi[l * 4 + j] for l in range(3))
+                               for i in range(2) for j in range(4)]
+        prods = [W.random_product(41, t, 2, 9, 8, 14) for t in range(24)]
+        trip = [(p.m, p.k, p.n, p.A, p.B) for p in prods]
+        want = [PK.digest(api.matmul(*t)) for t in trip]
+        saved = api.chunk_limbs()
+        api.set_chunk_limbs(1 << 12)  # several chunks: the pipelined path
+        try:
+            assert [PK.digest(c) for c in api.matmul_batch(trip)] == want
+        finally:
+            api.set_chunk_limbs(saved)
+        mats = [W.random_product(43, t, 3, 3, 10, 10) for t in range(4)]
+        X = api.chain([(3, 3, p.A) for p in mats])
+        M = mats[0].A.to_ints()
+        for p in mats[1:]:
+            B = p.A.to_ints()
+            M = [sum(M[i * 3 + l] * B[l * 3 + j] for l in range(3))
+                 for i in range(3) for j in range(3)]
+        assert X.to_ints() == M
+        srv = api.Server(slots=2, max_batch=8)
+        try:
+            tickets = [srv.submit(*t) for t in trip]
+            assert [PK.digest(srv.wait(t, 60000)) for t in tickets] == want
+        finally:
+            srv.close()
+    finally:
+        L.mpzmm_set_option(_lib.MPZMM_OPT_CHECK_BOUNDS, 0)
